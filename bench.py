@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Benchmark: FP64 net production rates + sparse reactor Jacobian (rate-eval states/s).
+
+Workload: seeded synthetic CHEMKIN mechanism with 53 species (C,H,O,N,Ar) and
+325 reactions (10% falloff, 15% third-body, 20% irreversible), 2^20
+independent states (T U[300,3000] K, log10 P U[0,2] atm, Y ~ Dirichlet(0.5)).
+One step = one fused pass over all states producing wdot [53] and the 1798
+Jacobian values of the 54x54 reactor Jacobian per state.  Inputs (445 MB) and
+outputs (15 GB) exceed the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun): every rank integrates its own 2^20 states (weak
+scaling, no collective on the data path); timing is the max over ranks.
+"""
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "c2_53"
+METRIC = "rate-eval states/s"
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--states", type=int, default=1 << 20)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 3 + i and r[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_per_state():
+    """DRAM bytes per state of the rates+Jacobian kernel from the committed
+    ncu summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", "rates_jac_c2_ncu.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("dram_bytes_per_state")
+    return None
+
+
+def make_workload(directory, n, seed):
+    from zerork_b200 import mechgen
+    g = mechgen.generate(mechgen.SPECS[WORKLOAD])
+    m, t = g.write(directory)
+    T, P, Y = mechgen.rate_states(g, n, seed=seed)
+    return g, (m, t), T, P, Y
+
+
+def cpu_reference(files, T, P, Y, budget_s=12.0, nthreads=None):
+    """The reference's own CPU mechanism library (oracle/_ref, default fmath exp
+    build) with the restated plugin Jacobian assembly, OpenMP over states."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import zrk_oracle as zo
+    kind = "fmath" if zo.ref_available("fmath") else "libc"
+    if not zo.ref_available(kind):
+        return None
+    nthreads = nthreads or os.cpu_count()
+    ref = zo.RefMechanism(files[0], files[1], kind=kind)
+    ot = zo.OracleTables(ref.tables)
+    # calibrate a bounded sample
+    m = 64 * nthreads
+    t0 = time.perf_counter()
+    ref.batch_rates_jac(files, ot, T[:m], P[:m], Y[:m], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    m2 = int(min(len(T), max(m, m * budget_s / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    ref.batch_rates_jac(files, ot, T[:m2], P[:m2], Y[:m2], nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return {"value": m2 / dt, "unit": "states/s", "cores": nthreads, "kind": "reference",
+            "sample": f"{m2} of the {len(T)} states, reference zerork::mechanism "
+                      f"({kind} exp) + restated SetupJacobianSparse, {nthreads} OpenMP threads"}
+
+
+def run_reference_arm(a, rank, world):
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as d:
+        g, files, T, P, Y = make_workload(d, min(a.states, 1 << 16), seed=7)
+        per_step = []
+        nthreads = os.cpu_count()
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import zrk_oracle as zo
+        kind = "fmath" if zo.ref_available("fmath") else "libc"
+        if not zo.ref_available(kind):
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "oracle/_ref not built (reference sources absent)"}))
+            return
+        ref = zo.RefMechanism(files[0], files[1], kind=kind)
+        ot = zo.OracleTables(ref.tables)
+        m = 96 * nthreads  # bounded sample per step
+        for i in range(a.warmup + a.steps):
+            lo = (i * m) % (len(T) - m)
+            t0 = time.perf_counter()
+            ref.batch_rates_jac(files, ot, T[lo:lo + m], P[lo:lo + m], Y[lo:lo + m],
+                                nthreads=nthreads)
+            if i >= a.warmup:
+                per_step.append(time.perf_counter() - t0)
+        ms = 1e3 * float(np.mean(per_step))
+        v = m / (ms / 1e3)
+        line = {"metric": METRIC, "value": v, "unit": "states/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+                "config": {"workload": "rates+jacobian, 53 species / 325 reactions, "
+                                       f"bounded sample of {m} states per step",
+                           "l2": "inputs per step exceed nothing on CPU"},
+                "cpu_baseline": {"value": v, "unit": "states/s", "cores": nthreads,
+                                 "kind": "reference",
+                                 "sample": f"{m} states per step, zerork::mechanism ({kind} exp)"
+                                           " + restated SetupJacobianSparse"},
+                "e2e": {"value": v, "unit": "states/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+
+
+def main():
+    a = args_()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if a.impl == "reference":
+        run_reference_arm(a, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import zerork_b200 as zb
+    dev = torch.device("cuda", local)
+    tmp = tempfile.TemporaryDirectory()
+    g, files, T, P, Y = make_workload(tmp.name, a.states, seed=7 + rank)
+    n = a.states
+    pm = zb.Mechanism(*files)
+    S, nnz = pm.nsp, pm.nnz
+    Td = torch.from_numpy(T).to(dev)
+    Pd = torch.from_numpy(P).to(dev)
+    Yd = torch.from_numpy(np.ascontiguousarray(Y.T)).to(dev)
+    W = torch.empty((S, n), dtype=torch.float64, device=dev)
+    J = torch.empty((nnz, n), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        pm.rates_jac(Td, Pd, Yd, W, J, stream=sptr)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(a.steps)]
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_end = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for i in range(a.steps):
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t_start.elapsed_time(t_end)
+    launch_ms = [e0.elapsed_time(e1) for e0, e1 in ev]
+    if world > 1:
+        tt = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        dist.barrier()
+    ms = total_ms / a.steps
+    value = world * n / (ms / 1e3)
+    # roofline of the (single) kernel per step
+    alg_bytes = n * 8 * ((S + 2) + S + nnz)
+    launch_avg = float(np.mean(launch_ms))
+    achieved = alg_bytes / (launch_avg / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    tps = traffic_per_state()
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": (tps * n if tps else None),
+            "peak_source": f"{peak_kind} hbm_gbs",
+            "algorithmic_bytes_per_state": 8 * ((S + 2) + S + nnz)}
+    # FP64-pipe roofline: transcendental count per state (two rate evaluations:
+    # at T and at the forward-difference temperature) at the measured exp rate
+    try:
+        fma_gflops, exp_gps = zb.measure_fp64()
+        fo_type = pm.table("fo_type")
+        troe_exps = int(np.sum(fo_type == 1) * 2 + np.sum(fo_type == 2) * 3)
+        per_eval = (len(pm.table("arr_step")) + len(pm.table("keq_step")) + len(fo_type) * 3
+                    + troe_exps + 2)
+        trans = 2 * per_eval
+        t_exp = trans * n / (exp_gps * 1e9)
+        roof["fp64"] = {"fma_gflops_measured": fma_gflops, "exp_g_per_s_measured": exp_gps,
+                        "transcendentals_per_state": trans,
+                        "exp_bound_ms": 1e3 * t_exp, "frac": 1e3 * t_exp / launch_avg}
+    except Exception as ex:  # diagnostics only
+        roof["fp64"] = {"error": str(ex)}
+    # end-to-end through the host C-ABI entry (pinned host buffers)
+    e2e = None
+    if not a.no_e2e:
+        Th = torch.from_numpy(T).pin_memory()
+        Ph = torch.from_numpy(P).pin_memory()
+        Yh = torch.from_numpy(np.ascontiguousarray(Y.T)).pin_memory()
+        Wh = torch.empty((S, n), dtype=torch.float64).pin_memory()
+        Jh = torch.empty((nnz, n), dtype=torch.float64).pin_memory()
+        L = zb.lib()
+
+        def e2e_step():
+            zb.check(L.zrk_rates_jac_host(pm.handle, n, zb._ptr(Th), zb._ptr(Ph), zb._ptr(Yh),
+                                          zb._ptr(Wh), zb._ptr(Jh)))
+        e2e_step()
+        e2e_steps = max(2, min(a.steps, 5))
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        dt = (time.perf_counter() - t0) / e2e_steps
+        if world > 1:
+            tt = torch.tensor([dt], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            dt = float(tt.item())
+        e2e = {"value": world * n / dt, "unit": "states/s",
+               "h2d_bytes_per_step": int(Th.nbytes + Ph.nbytes + Yh.nbytes),
+               "d2h_bytes_per_step": int(Wh.nbytes + Jh.nbytes), "steps": e2e_steps}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu:
+        cpu = cpu_reference(files, T, P, Y)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "states/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic (seeded mechanism and states)",
+                "config": {"workload": "rates+jacobian: 53 species / 325 reactions / "
+                                       f"{pm.nstep} steps, {n} states per GPU, nnz {nnz}",
+                           "global_states": world * n, "parallelism": f"shard{world}",
+                           "l2": "inputs 445 MB + outputs 15 GB per step exceed L2; no flush",
+                           "launch": pm.get_launch()},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": a.steps, "clocks": clk.summary()}
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,101 @@
+/*
+ * zerork_b200.h -- C ABI of the sm_100a mechanism kernels (mechanism level).
+ *
+ * Plain pointers and sizes only.  Device arrays are species-major
+ * (structure of arrays): x[item * ld + state], ld >= n, the layout of
+ * zerork::mechanism_cuda's multi-reactor entry points
+ * (src/zerork/mechanism_cuda.h:19-45, C[j * nReactors + k]).
+ * Every function returns 0 on success and a nonzero zerork_b200 error code
+ * otherwise; zrk_last_error() gives the message of the calling thread.
+ */
+#ifndef ZERORK_B200_H
+#define ZERORK_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct zrk_mech_impl *zrk_mech_t;
+
+enum {
+  ZRK_OK = 0,
+  ZRK_ERR_INVALID_HANDLE = 1,
+  ZRK_ERR_INVALID_POINTER = 2,
+  ZRK_ERR_PARSE = 3,
+  ZRK_ERR_CUDA = 4,
+  ZRK_ERR_INVALID_ARGUMENT = 5,
+  ZRK_ERR_NO_DEVICE = 6
+};
+
+/* Last error message of the calling thread (never NULL). */
+const char *zrk_last_error(void);
+
+/* Parse a CHEMKIN mechanism + thermo file pair and upload the tables to the
+ * current CUDA device.  Replaces zerork::mechanism::mechanism(mech, therm,
+ * log) (src/zerork/mechanism.h:23-27) plus mechanism_cuda's table upload
+ * (src/zerork/mechanism_cuda.h:12-17).  Errors: ZRK_ERR_PARSE (unsupported
+ * or malformed input), ZRK_ERR_NO_DEVICE, ZRK_ERR_CUDA. */
+int zrk_mech_create(const char *mech_file, const char *therm_file, zrk_mech_t *out);
+int zrk_mech_free(zrk_mech_t m);
+
+/* Parse only (no device upload): the tables and Jacobian pattern can be
+ * inspected, kernel entry points return ZRK_ERR_NO_DEVICE. */
+int zrk_mech_parse(const char *mech_file, const char *therm_file, zrk_mech_t *out);
+
+/* Sizes: getNumSpecies/getNumReactions/getNumSteps (mechanism.h:30-34) and
+ * the Jacobian nonzero count of the (nsp+1)^2 reactor Jacobian
+ * (applications/cfd_plugin/reactor_nvector_serial.cpp:214-232). */
+int zrk_mech_sizes(zrk_mech_t m, int *nsp, int *nrxn, int *nstep, int *nnz);
+
+/* Export one mechanism table by name (e.g. "mw", "arr_lnA", "reac_spc"),
+ * the tables zerork::rate_const / info_net build internally
+ * (src/zerork/rate_const.h:98-170).  *count receives the element count; data
+ * is copied when out != NULL and capacity >= count.  is_double says whether
+ * elements are double (1) or int32 (0). */
+int zrk_mech_table(zrk_mech_t m, const char *name, void *out, long capacity, long *count,
+                   int *is_double);
+
+/* Species name (getSpeciesName, mechanism.h:55). */
+const char *zrk_mech_species_name(zrk_mech_t m, int idx);
+
+/* Fixed Jacobian pattern, compressed column over nsp+1 variables:
+ * col_ptr[nsp+2], row_idx[nnz]; SetupSparseJacobianArrays
+ * (applications/cfd_plugin/reactor_nvector_serial.cpp:122-281). */
+int zrk_mech_jac_pattern(zrk_mech_t m, int *col_ptr, int *row_idx);
+
+/* Options used by the kernels (defaults as the cfd_plugin,
+ * zerork_reactor_manager.cpp:49-101): "reference_temperature" (1.0),
+ * "min_mass_fraction" (1e-30), "step_limiter" (1e22). */
+int zrk_mech_set_double_option(zrk_mech_t m, const char *name, double value);
+int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value);
+
+/* Tile mapping of the rate kernel: ts states per tile (8/16/32), warps per
+ * CTA (1..16), global_ws = 1 puts the per-tile workspace in global scratch
+ * (grid CTAs; 0 = one CTA per tile).  ts = 0 selects the autotuned mapping. */
+int zrk_mech_set_launch(zrk_mech_t m, int ts, int warps, int global_ws, int grid);
+int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *warps, int *global_ws, int *grid);
+
+/* Net production rates + reactor Jacobian at independent (T, P, Y) states,
+ * all device pointers on the current device, species-major with leading
+ * dimension ld.  Per state: inverse density from (T, P, Y); y = [Y, T/Tref];
+ * wdot = net production rates (getReactionRatesLimiter, mechanism.h:143);
+ * jac = SetupJacobianSparse values (reactor_nvector_serial.cpp:610-771)
+ * in compressed-column order, [nnz][ld]; ydot = GetTimeDerivative
+ * (reactor_constant_volume_cpu.cpp:64-128), [nsp+1][ld].  jac and ydot may
+ * be NULL.  stream is a cudaStream_t (NULL = legacy default stream).  The
+ * call is asynchronous; scratch needed by the global-workspace mapping is
+ * allocated by the library on first use and shared by all calls on the
+ * handle, so with that mapping calls on one handle must not overlap on the
+ * GPU (use one stream or one handle per stream). */
+int zrk_rates_jac_dev(zrk_mech_t m, int n, int ld, const double *T, const double *P,
+                      const double *Y, double *wdot, double *jac, double *ydot, void *stream);
+
+/* Same with host buffers (species-major, ld = n): copies in, computes,
+ * copies out, synchronizes.  Host buffers may be pageable or pinned. */
+int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, const double *Y,
+                       double *wdot, double *jac);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

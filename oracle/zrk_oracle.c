@@ -1,0 +1,549 @@
+/*
+ * zrk_oracle.c -- CPU ORACLE (test infrastructure only; see zrk_oracle.h).
+ *
+ * Restates, operation for operation, the reference's CPU rate path so that it
+ * agrees with the reference library built with ZERORK_EXP_LIBC to rounding.
+ * Citations are to files of the Zero-RK checkout.
+ */
+#include "zrk_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static void *zcalloc(size_t n, size_t sz) { return calloc(n > 0 ? n : 1, sz); }
+
+zo_tables *zo_tables_alloc(const int s[11]) {
+  zo_tables *t = (zo_tables *)zcalloc(1, sizeof(zo_tables));
+  t->nsp = s[0]; t->nrxn = s[1]; t->nstep = s[2];
+  t->tot_reac = s[3]; t->tot_prod = s[4];
+  t->n_arr = s[5]; t->n_keq = s[6]; t->n_tb = s[7]; t->n_fo = s[8];
+  t->n_tb_eff = s[9]; t->n_fo_eff = s[10];
+  t->mw = (double *)zcalloc(t->nsp, sizeof(double));
+  t->thermo = (double *)zcalloc((size_t)t->nsp * 16, sizeof(double));
+  t->step_rxn = (int *)zcalloc(t->nstep, sizeof(int));
+  t->step_dir = (int *)zcalloc(t->nstep, sizeof(int));
+  t->reac_ptr = (int *)zcalloc(t->nstep + 1, sizeof(int));
+  t->reac_spc = (int *)zcalloc(t->tot_reac, sizeof(int));
+  t->prod_ptr = (int *)zcalloc(t->nstep + 1, sizeof(int));
+  t->prod_spc = (int *)zcalloc(t->tot_prod, sizeof(int));
+  t->arr_step = (int *)zcalloc(t->n_arr, sizeof(int));
+  t->arr_lnA = (double *)zcalloc(t->n_arr, sizeof(double));
+  t->arr_n = (double *)zcalloc(t->n_arr, sizeof(double));
+  t->arr_Ta = (double *)zcalloc(t->n_arr, sizeof(double));
+  t->keq_step = (int *)zcalloc(t->n_keq, sizeof(int));
+  t->keq_fwd = (int *)zcalloc(t->n_keq, sizeof(int));
+  t->keq_dn = (double *)zcalloc(t->n_keq, sizeof(double));
+  t->tb_fwd = (int *)zcalloc(t->n_tb, sizeof(int));
+  t->tb_rev = (int *)zcalloc(t->n_tb, sizeof(int));
+  t->tb_ptr = (int *)zcalloc(t->n_tb + 1, sizeof(int));
+  t->tb_spc = (int *)zcalloc(t->n_tb_eff, sizeof(int));
+  t->tb_alpha = (double *)zcalloc(t->n_tb_eff, sizeof(double));
+  t->fo_fwd = (int *)zcalloc(t->n_fo, sizeof(int));
+  t->fo_rev = (int *)zcalloc(t->n_fo, sizeof(int));
+  t->fo_type = (int *)zcalloc(t->n_fo, sizeof(int));
+  t->fo_spc = (int *)zcalloc(t->n_fo, sizeof(int));
+  t->fo_ptr = (int *)zcalloc(t->n_fo + 1, sizeof(int));
+  t->fo_eff_spc = (int *)zcalloc(t->n_fo_eff, sizeof(int));
+  t->fo_alpha = (double *)zcalloc(t->n_fo_eff, sizeof(double));
+  t->fo_par = (double *)zcalloc((size_t)t->n_fo * 8, sizeof(double));
+  return t;
+}
+
+void zo_tables_free(zo_tables *t) {
+  if (!t) return;
+  free(t->mw); free(t->thermo); free(t->step_rxn); free(t->step_dir);
+  free(t->reac_ptr); free(t->reac_spc); free(t->prod_ptr); free(t->prod_spc);
+  free(t->arr_step); free(t->arr_lnA); free(t->arr_n); free(t->arr_Ta);
+  free(t->keq_step); free(t->keq_fwd); free(t->keq_dn);
+  free(t->tb_fwd); free(t->tb_rev); free(t->tb_ptr); free(t->tb_spc); free(t->tb_alpha);
+  free(t->fo_fwd); free(t->fo_rev); free(t->fo_type); free(t->fo_spc); free(t->fo_ptr);
+  free(t->fo_eff_spc); free(t->fo_alpha); free(t->fo_par);
+  free(t);
+}
+
+/* ------------------------------------------------------------------ thermo */
+/* nasa_poly.cpp:50-76 getCp_R */
+void zo_cp_R(const zo_tables *t, double T, double *cp_R) {
+  for (int j = 0; j < t->nsp; ++j) {
+    const double *c = t->thermo + 16 * j;
+    if (T < c[0])
+      cp_R[j] = c[1] + T * (c[2] + T * (c[3] + T * (c[4] + T * c[5])));
+    else
+      cp_R[j] = c[8] + T * (c[9] + T * (c[10] + T * (c[11] + T * c[12])));
+  }
+}
+
+/* nasa_poly.cpp:78-117 getH_RT */
+void zo_h_RT(const zo_tables *t, double T, double *h_RT) {
+  double invT = 1.0 / T, m[4];
+  m[0] = T; m[1] = T * m[0]; m[2] = T * m[1]; m[3] = T * m[2];
+  m[0] *= 0.50000000000000000000;
+  m[1] *= 0.33333333333333333333;
+  m[2] *= 0.25000000000000000000;
+  m[3] *= 0.20000000000000000000;
+  for (int j = 0; j < t->nsp; ++j) {
+    const double *c = t->thermo + 16 * j;
+    if (T < c[0])
+      h_RT[j] = c[1] + c[2] * m[0] + c[3] * m[1] + c[4] * m[2] + c[5] * m[3] + c[6] * invT;
+    else
+      h_RT[j] = c[8] + c[9] * m[0] + c[10] * m[1] + c[11] * m[2] + c[12] * m[3] + c[13] * invT;
+  }
+}
+
+/* nasa_poly.cpp:118-172 getG_RT */
+void zo_g_RT(const zo_tables *t, double T, double *g_RT) {
+  double invT = 1.0 / T, m[5];
+  m[0] = 1.0 - log(T);
+  m[1] = T; m[2] = T * m[1]; m[3] = T * m[2]; m[4] = T * m[3];
+  m[1] *= -0.50000000000000000000;
+  m[2] *= -0.16666666666666666667;
+  m[3] *= -0.08333333333333333333;
+  m[4] *= -0.05000000000000000000;
+  for (int j = 0; j < t->nsp; ++j) {
+    const double *c = t->thermo + 16 * j;
+    if (T < c[0])
+      g_RT[j] = c[1] * m[0] + c[2] * m[1] + c[3] * m[2] + c[4] * m[3] + c[5] * m[4] +
+                c[6] * invT - c[7];
+    else
+      g_RT[j] = c[8] * m[0] + c[9] * m[1] + c[10] * m[2] + c[11] * m[3] + c[12] * m[4] +
+                c[13] * invT - c[14];
+  }
+}
+
+/* ------------------------------------------------------- rate coefficients */
+/* rate_const.cpp:539-582 updateK, with updateArrheniusStep (:669-687),
+ * updateFromKeqStep (:690-731), updateThirdBodyRxn (:862-888) and
+ * updateFalloffRxn (:890-1012).  Exponentials use libc exp (the
+ * ZERORK_EXP_LIBC build, fast_exps.cpp). */
+void zo_rate_coefs(const zo_tables *t, double T, const double *C, double *K) {
+  const int nsp = t->nsp;
+  for (int j = 0; j < t->nstep; ++j) K[j] = 0.0;
+  const double logT = log(T);
+  const double invT = 1.0 / T;
+  const double log_PatmInvRuT = log(ZO_PATM / (ZO_RU * T));
+  double Csum = 0.0;
+  for (int j = 0; j < nsp; ++j) Csum += C[j];
+
+  for (int j = 0; j < t->n_arr; ++j) {
+    double a = t->arr_lnA[j] + t->arr_n[j] * logT - t->arr_Ta[j] * invT;
+    K[t->arr_step[j]] = exp(a);
+  }
+  if (t->n_keq > 0) {
+    double *g = (double *)malloc(sizeof(double) * nsp);
+    zo_g_RT(t, T, g);
+    for (int j = 0; j < t->n_keq; ++j) {
+      const int f = t->keq_fwd[j];
+      double s = 0.0;
+      for (int k = t->prod_ptr[f]; k < t->prod_ptr[f + 1]; ++k) s += g[t->prod_spc[k]];
+      for (int k = t->reac_ptr[f]; k < t->reac_ptr[f + 1]; ++k) s -= g[t->reac_spc[k]];
+      double keq = exp(s - t->keq_dn[j] * log_PatmInvRuT);
+      K[t->keq_step[j]] = keq * K[f];
+    }
+    free(g);
+  }
+  for (int j = 0; j < t->n_tb; ++j) {
+    double Cmult = Csum;
+    for (int k = t->tb_ptr[j]; k < t->tb_ptr[j + 1]; ++k) Cmult += C[t->tb_spc[k]] * t->tb_alpha[k];
+    K[t->tb_fwd[j]] *= Cmult;
+    if (t->tb_rev[j] >= 0) K[t->tb_rev[j]] *= Cmult;
+  }
+  for (int j = 0; j < t->n_fo; ++j) {
+    const double *p = t->fo_par + 8 * j;
+    double Klow = exp(p[0] + p[1] * logT - p[2] * invT);
+    double Cmult;
+    if (t->fo_spc[j] >= 0) {
+      Cmult = C[t->fo_spc[j]];
+    } else {
+      Cmult = Csum;
+      for (int k = t->fo_ptr[j]; k < t->fo_ptr[j + 1]; ++k)
+        Cmult += C[t->fo_eff_spc[k]] * t->fo_alpha[k];
+    }
+    double Pr = Klow * Cmult / K[t->fo_fwd[j]];
+    if (Pr < 1.0e-300) Pr = 1.0e-300;
+    double lPr = log10(Pr);
+    double fTerm = 1.0;
+    const int ty = t->fo_type[j];
+    if (ty == ZO_FO_TROE3 || ty == ZO_FO_TROE4) {
+      double Fc = 0.0;
+      if (p[4] != 0) Fc += (1.0 - p[3]) * exp(-T / p[4]);
+      if (p[5] != 0) Fc += p[3] * exp(-T / p[5]);
+      if (ty == ZO_FO_TROE4) Fc += exp(-p[6] * invT);
+      if (Fc < 1.0e-300) Fc = 1.0e-300;
+      fTerm = log10(Fc);
+      double nTerm = 0.75 - 1.27 * fTerm;
+      lPr -= (0.4 + 0.67 * fTerm);
+      lPr = lPr / (nTerm - 0.14 * lPr);
+      lPr *= lPr;
+      fTerm /= (1.0 + lPr);
+      fTerm = pow(10.0, fTerm);
+    } else if (ty == ZO_FO_SRI) {
+      const double x_power = 1.0 / (1.0 + lPr * lPr);
+      fTerm = p[3] * exp(-p[4] * invT);
+      if (p[5] > 0) fTerm += exp(-T * p[5]);
+      fTerm = pow(fTerm, x_power);
+      fTerm *= p[6];
+      fTerm *= pow(T, p[7]);
+    }
+    double Pcorr = fTerm * Pr / (1.0 + Pr);
+    K[t->fo_fwd[j]] *= Pcorr;
+    if (t->fo_rev[j] >= 0) K[t->fo_rev[j]] *= Pcorr;
+  }
+}
+
+/* perf_net.cpp:190-274 calcRatesFromTC_StepLimiter (lim != NULL) and
+ * perf_net.cpp:126-188 calcRatesFromTC (lim == NULL). */
+void zo_rates(const zo_tables *t, double T, const double *C, const double *lim,
+              double *net, double *cre, double *des, double *rop) {
+  zo_rate_coefs(t, T, C, rop);
+  if (lim) {
+    for (int j = 0; j < t->nstep; ++j)
+      if (0.0 < lim[j] && lim[j] < 1.0e+300) rop[j] *= lim[j] / (lim[j] + rop[j]);
+  }
+  for (int j = 0; j < t->nstep; ++j)
+    for (int k = t->reac_ptr[j]; k < t->reac_ptr[j + 1]; ++k) rop[j] *= C[t->reac_spc[k]];
+  memset(cre, 0, sizeof(double) * t->nsp);
+  memset(des, 0, sizeof(double) * t->nsp);
+  for (int j = 0; j < t->nstep; ++j)
+    for (int k = t->reac_ptr[j]; k < t->reac_ptr[j + 1]; ++k) des[t->reac_spc[k]] += rop[j];
+  for (int j = 0; j < t->nstep; ++j)
+    for (int k = t->prod_ptr[j]; k < t->prod_ptr[j + 1]; ++k) cre[t->prod_spc[k]] += rop[j];
+  for (int j = 0; j < t->nsp; ++j) net[j] = cre[j] - des[j];
+}
+
+/* ------------------------------------------ oracle kinetics provider */
+static void ok_rates(void *ctx, double T, const double *C, const double *lim, double *net,
+                     double *cre, double *des, double *rop) {
+  zo_rates((const zo_tables *)ctx, T, C, lim, net, cre, des, rop);
+}
+/* mechanism.cpp:374-379 getIntEnergy_RT */
+static void ok_u_RT(void *ctx, double T, double *u) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  zo_h_RT(t, T, u);
+  for (int j = 0; j < t->nsp; ++j) u[j] -= 1.0;
+}
+/* mechanism.cpp:421-434 getMassCvFromTY */
+static double ok_mass_cv(void *ctx, double T, const double *y, double *cv) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double mix = 0.0;
+  zo_cp_R(t, T, cv);
+  for (int j = 0; j < t->nsp; ++j) {
+    cv[j] -= 1.0;
+    cv[j] *= ZO_RU / t->mw[j];
+    mix += cv[j] * y[j];
+  }
+  return mix;
+}
+/* mechanism.cpp:267-283 getMolWtMixFromY / getDensityFromTPY */
+static double ok_density(void *ctx, double T, double P, const double *y) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double s = 0.0;
+  for (int j = 0; j < t->nsp; ++j) s += y[j] * (1.0 / t->mw[j]);
+  double mwmix = 1.0 / s;
+  return P * mwmix / (ZO_RU * T);
+}
+/* mechanism.cpp:321-327 getCfromVY */
+static void ok_c_from_vy(void *ctx, double v, const double *y, double *c) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double dens = 1.0 / v;
+  for (int j = 0; j < t->nsp; ++j) c[j] = dens * (1.0 / t->mw[j]) * y[j];
+}
+
+void zo_kinetics_oracle(const zo_tables *t, zo_kinetics *k) {
+  k->ctx = (void *)t;
+  k->rates_limiter = ok_rates;
+  k->int_energy_RT = ok_u_RT;
+  k->mass_cv = ok_mass_cv;
+  k->density_TPY = ok_density;
+  k->c_from_vy = ok_c_from_vy;
+}
+
+/* ------------------------------------------------------------- reactor */
+zo_reactor *zo_reactor_new(const zo_tables *t, const zo_kinetics *kin, double Tref,
+                           double min_mass_frac, double step_limiter) {
+  zo_reactor *r = (zo_reactor *)zcalloc(1, sizeof(zo_reactor));
+  r->t = t;
+  r->kin = *kin;
+  r->nsp = t->nsp;
+  r->nstep = t->nstep;
+  r->Tref = Tref;
+  r->min_mass_frac = min_mass_frac;
+  r->inv_density = 1.0;
+  const int n = t->nsp, m = t->nstep;
+  r->lim = (double *)zcalloc(m, sizeof(double));
+  for (int j = 0; j < m; ++j) r->lim[j] = step_limiter; /* reactor_nvector_serial.cpp:56 */
+  r->C = (double *)zcalloc(n, sizeof(double));
+  r->net = (double *)zcalloc(n, sizeof(double));
+  r->cre = (double *)zcalloc(n, sizeof(double));
+  r->des = (double *)zcalloc(n, sizeof(double));
+  r->rop = (double *)zcalloc(m, sizeof(double));
+  r->u_RT = (double *)zcalloc(n, sizeof(double));
+  r->cv_spc = (double *)zcalloc(n, sizeof(double));
+  r->tmp1 = (double *)zcalloc(n + 1, sizeof(double));
+  r->tmp2 = (double *)zcalloc(n + 1, sizeof(double));
+  r->tmp3 = (double *)zcalloc(n + 1, sizeof(double));
+  r->yscale = (double *)zcalloc(n + 1, sizeof(double));
+  r->fscale = (double *)zcalloc(n + 1, sizeof(double));
+  return r;
+}
+
+void zo_reactor_free(zo_reactor *r) {
+  if (!r) return;
+  free(r->lim); free(r->C); free(r->net); free(r->cre); free(r->des); free(r->rop);
+  free(r->u_RT); free(r->cv_spc); free(r->tmp1); free(r->tmp2); free(r->tmp3);
+  free(r->yscale); free(r->fscale);
+  free(r);
+}
+
+/* reactor_constant_volume_cpu.cpp:27 */
+void zo_reactor_set_density(zo_reactor *r, double T, double P, const double *Y) {
+  r->inv_density = 1.0 / r->kin.density_TPY(r->kin.ctx, T, P, Y);
+}
+
+/* reactor_constant_volume_cpu.cpp:64-128 GetTimeDerivative, with no
+ * energy/pressure/mass sources (dpdt = e_src = 0, y_src = NULL). */
+int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot) {
+  const int n = r->nsp;
+  double T = y[n] * r->Tref;
+  if (T <= 0.0) return 1;
+  if (T > 1.0e4) T = 1.0e4;
+  r->kin.int_energy_RT(r->kin.ctx, T, r->u_RT);
+  r->mean_cv = r->kin.mass_cv(r->kin.ctx, T, y, r->cv_spc);
+  const double v = r->inv_density;
+  r->kin.c_from_vy(r->kin.ctx, v, y, r->C);
+  r->kin.rates_limiter(r->kin.ctx, T, r->C, r->lim, r->net, r->cre, r->des, r->rop);
+  double esum = 0.0;
+  for (int j = 0; j < n; ++j) {
+    ydot[j] = (r->net[j] * r->t->mw[j] * v);
+    esum += r->u_RT[j] * r->net[j] * v;
+  }
+  double dT_dt = -esum * ZO_RU * y[n] / r->mean_cv;
+  ydot[n] = dT_dt + (0.0 + 0.0 * v) / (r->mean_cv * r->Tref);
+  double es = 0.0;
+  for (int j = 0; j < n; ++j) {
+    double m = fabs(r->cre[j]) + fabs(r->des[j]);
+    r->yscale[j] = m * r->t->mw[j] * v;
+    es += fabs(r->u_RT[j]) * m * v;
+  }
+  r->yscale[n] = es * ZO_RU * fabs(y[n]) / fabs(r->mean_cv);
+  return 0;
+}
+
+/* ------------------------------------------------------ Jacobian pattern */
+/* reactor_nvector_serial.cpp:122-281 SetupSparseJacobianArrays */
+zo_jac_pattern *zo_jac_pattern_new(const zo_tables *t) {
+  const int ns = t->nsp, nv = ns + 1;
+  int *nzf = (int *)zcalloc((size_t)nv * nv, sizeof(int)); /* [col*nv+row] */
+  for (int j = 0; j < ns; ++j) {
+    nzf[j * nv + j] = 1;
+    nzf[j * nv + ns] = 1;
+  }
+  for (int k = 0; k < nv; ++k) nzf[ns * nv + k] = 1;
+  int nd = 0, nc = 0;
+  for (int j = 0; j < t->nstep; ++j) {
+    int nr = t->reac_ptr[j + 1] - t->reac_ptr[j];
+    int np = t->prod_ptr[j + 1] - t->prod_ptr[j];
+    nd += nr * nr;
+    nc += nr * np;
+  }
+  zo_jac_pattern *p = (zo_jac_pattern *)zcalloc(1, sizeof(zo_jac_pattern));
+  p->n = nv;
+  p->n_des = nd;
+  p->n_cre = nc;
+  p->des_conc = (int *)zcalloc(nd, sizeof(int));
+  p->des_step = (int *)zcalloc(nd, sizeof(int));
+  p->des_nz = (int *)zcalloc(nd, sizeof(int));
+  p->cre_conc = (int *)zcalloc(nc, sizeof(int));
+  p->cre_step = (int *)zcalloc(nc, sizeof(int));
+  p->cre_nz = (int *)zcalloc(nc, sizeof(int));
+  int id = 0, ic = 0;
+  for (int j = 0; j < t->nstep; ++j) {
+    for (int k = t->reac_ptr[j]; k < t->reac_ptr[j + 1]; ++k) {
+      int col = t->reac_spc[k];
+      for (int m = t->reac_ptr[j]; m < t->reac_ptr[j + 1]; ++m) {
+        int row = t->reac_spc[m];
+        nzf[col * nv + row] = 1;
+        p->des_conc[id] = col; p->des_step[id] = j; p->des_nz[id] = row; ++id;
+      }
+      for (int m = t->prod_ptr[j]; m < t->prod_ptr[j + 1]; ++m) {
+        int row = t->prod_spc[m];
+        nzf[col * nv + row] = 1;
+        p->cre_conc[ic] = col; p->cre_step[ic] = j; p->cre_nz[ic] = row; ++ic;
+      }
+    }
+  }
+  int cnt = 1;
+  p->col_ptr = (int *)zcalloc(nv + 1, sizeof(int));
+  for (int j = 0; j < nv; ++j) {
+    for (int k = 0; k < nv; ++k)
+      if (nzf[j * nv + k] == 1) nzf[j * nv + k] = cnt++;
+    p->col_ptr[j + 1] = cnt - 1;
+  }
+  p->nnz = cnt - 1;
+  p->row_idx = (int *)zcalloc(p->nnz, sizeof(int));
+  p->last_row = (int *)zcalloc(nv, sizeof(int));
+  for (int j = 0; j < nv; ++j) {
+    for (int k = 0; k < nv; ++k) {
+      int a = nzf[j * nv + k];
+      if (a > 0) p->row_idx[a - 1] = k;
+    }
+    p->last_row[j] = nzf[(j + 1) * nv - 1] - 1;
+  }
+  for (int i = 0; i < nd; ++i) p->des_nz[i] = nzf[p->des_conc[i] * nv + p->des_nz[i]] - 1;
+  for (int i = 0; i < nc; ++i) p->cre_nz[i] = nzf[p->cre_conc[i] * nv + p->cre_nz[i]] - 1;
+  free(nzf);
+  return p;
+}
+
+void zo_jac_pattern_free(zo_jac_pattern *p) {
+  if (!p) return;
+  free(p->col_ptr); free(p->row_idx); free(p->last_row);
+  free(p->des_conc); free(p->des_step); free(p->des_nz);
+  free(p->cre_conc); free(p->cre_step); free(p->cre_nz);
+  free(p);
+}
+
+/* reactor_nvector_serial.cpp:610-771 SetupJacobianSparse (integer network,
+ * temperature solved).  UNIT_ROUNDOFF is DBL_EPSILON (SUNDIALS realtype). */
+int zo_jac_values(zo_reactor *r, const zo_jac_pattern *p, const double *y, const double *fy,
+                  double *jac, double *scale) {
+  const int ns = r->nsp, nv = ns + 1;
+  const double *mw = r->t->mw;
+  double *t1 = r->tmp1, *t2 = r->tmp2, *t3 = r->tmp3;
+  const double mmf = r->min_mass_frac;
+  const double sqrt_ur = sqrt(2.2204460492503131e-16);
+  for (int j = 0; j < ns; ++j) {
+    t1[j] = y[j];
+    if (fabs(t1[j]) < mmf) t1[j] = (t1[j] < 0.0) ? -mmf : mmf;
+    t2[j] = mw[j] / t1[j] * r->inv_density;
+  }
+  t1[ns] = y[ns];
+  if (zo_cv_rhs(r, t1, t3)) return 1;
+  for (int k = 0; k < p->nnz; ++k) jac[k] = 0.0;
+  if (scale)
+    for (int k = 0; k < p->nnz; ++k) scale[k] = 0.0;
+  for (int i = 0; i < p->n_des; ++i) {
+    double v = r->rop[p->des_step[i]] * t2[p->des_conc[i]];
+    jac[p->des_nz[i]] -= v;
+    if (scale) scale[p->des_nz[i]] += fabs(v);
+  }
+  for (int i = 0; i < p->n_cre; ++i) {
+    double v = r->rop[p->cre_step[i]] * t2[p->cre_conc[i]];
+    jac[p->cre_nz[i]] += v;
+    if (scale) scale[p->cre_nz[i]] += fabs(v);
+  }
+  /* d(Tdot)/dy_j */
+  const double RuTemp = ZO_RU * y[ns];
+  for (int j = 0; j < ns; ++j) {
+    int lr = p->last_row[j];
+    jac[lr] = 0.0;
+    double sc = 0.0;
+    for (int k = p->col_ptr[j]; k < p->col_ptr[j + 1] - 1; ++k) {
+      jac[lr] += jac[k] * r->u_RT[p->row_idx[k]];
+      if (scale) sc += scale[k] * fabs(r->u_RT[p->row_idx[k]]);
+    }
+    jac[lr] *= RuTemp;
+    if (scale) scale[lr] = sc * fabs(RuTemp);
+  }
+  for (int j = 0; j < ns; ++j) {
+    int lr = p->last_row[j];
+    double add = t3[ns] * r->cv_spc[j] * mw[j];
+    jac[lr] += add;
+    if (scale) scale[lr] += fabs(add);
+  }
+  const double multFact = -1.0 / (r->mean_cv);
+  for (int j = 0; j < ns; ++j) {
+    int lr = p->last_row[j];
+    jac[lr] *= (1.0 / mw[j]) * multFact;
+    if (scale) scale[lr] *= fabs((1.0 / mw[j]) * multFact);
+  }
+  /* d(ydot)/dT by forward difference */
+  double dT = y[ns] * sqrt_ur;
+  t1[ns] += dT;
+  dT = t1[ns] - y[ns];
+  const double mult = 1.0 / dT;
+  for (int j = 0; j < ns; ++j) t1[j] = y[j];
+  if (zo_cv_rhs(r, t1, t3)) return 1;
+  for (int k = p->col_ptr[ns]; k < p->col_ptr[nv]; ++k) {
+    int row = p->row_idx[k];
+    jac[k] = (t3[row] - fy[row]) * mult;
+    /* forward-difference rounding scale: term magnitudes of both RHS / dT */
+    if (scale) scale[k] = (r->yscale[row] + r->fscale[row]) * fabs(mult);
+  }
+  /* dC -> dY conversion */
+  for (int j = 0; j < ns; ++j) {
+    for (int k = p->col_ptr[j]; k < p->col_ptr[j + 1]; ++k) {
+      const int row = p->row_idx[k];
+      if (row < ns) {
+        jac[k] *= mw[row] * (1.0 / mw[j]);
+        if (scale) scale[k] *= mw[row] * (1.0 / mw[j]);
+      }
+    }
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------- batched driver */
+int zo_batch_rates_jac(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kins,
+                       int nthreads, int nstates, const double *T, const double *P,
+                       const double *Y, double Tref, double min_mass_frac,
+                       double step_limiter, double *wdot, double *jac, double *ydot) {
+  const int ns = t->nsp, nv = ns + 1;
+  int nfail = 0;
+  if (nthreads < 1) nthreads = 1;
+#pragma omp parallel num_threads(nthreads) reduction(+ : nfail)
+  {
+    int tid = 0, nth = 1;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+    nth = omp_get_num_threads();
+#endif
+    zo_reactor *r = zo_reactor_new(t, &kins[tid], Tref, min_mass_frac, step_limiter);
+    double *y = (double *)zcalloc(nv, sizeof(double));
+    double *fy = (double *)zcalloc(nv, sizeof(double));
+    long lo = (long)nstates * tid / nth, hi = (long)nstates * (tid + 1) / nth;
+    for (long s = lo; s < hi; ++s) {
+      const double *Ys = Y + s * ns;
+      zo_reactor_set_density(r, T[s], P[s], Ys);
+      for (int j = 0; j < ns; ++j) y[j] = Ys[j];
+      y[ns] = T[s] / Tref;
+      if (zo_cv_rhs(r, y, fy)) { ++nfail; continue; }
+      if (wdot) memcpy(wdot + s * ns, r->net, sizeof(double) * ns);
+      if (ydot) memcpy(ydot + s * nv, fy, sizeof(double) * nv);
+      if (jac && zo_jac_values(r, p, y, fy, jac + s * (long)p->nnz, NULL)) ++nfail;
+    }
+    free(y); free(fy);
+    zo_reactor_free(r);
+  }
+  return nfail;
+}
+
+int zo_batch_rates_jac_scaled(const zo_tables *t, const zo_jac_pattern *p, int nstates,
+                              const double *T, const double *P, const double *Y, double Tref,
+                              double min_mass_frac, double step_limiter, double *wdot,
+                              double *jac, double *wscale, double *jscale) {
+  const int ns = t->nsp, nv = ns + 1;
+  zo_kinetics kin;
+  zo_kinetics_oracle(t, &kin);
+  zo_reactor *r = zo_reactor_new(t, &kin, Tref, min_mass_frac, step_limiter);
+  double *y = (double *)zcalloc(nv, sizeof(double));
+  double *fy = (double *)zcalloc(nv, sizeof(double));
+  int nfail = 0;
+  for (long s = 0; s < nstates; ++s) {
+    const double *Ys = Y + s * ns;
+    zo_reactor_set_density(r, T[s], P[s], Ys);
+    for (int j = 0; j < ns; ++j) y[j] = Ys[j];
+    y[ns] = T[s] / Tref;
+    if (zo_cv_rhs(r, y, fy)) { ++nfail; continue; }
+    memcpy(wdot + s * ns, r->net, sizeof(double) * ns);
+    for (int j = 0; j < ns; ++j) wscale[s * ns + j] = fabs(r->cre[j]) + fabs(r->des[j]);
+    memcpy(r->fscale, r->yscale, sizeof(double) * nv);
+    if (zo_jac_values(r, p, y, fy, jac + s * (long)p->nnz, jscale + s * (long)p->nnz)) ++nfail;
+  }
+  free(y); free(fy);
+  zo_reactor_free(r);
+  return nfail;
+}

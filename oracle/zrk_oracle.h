@@ -1,0 +1,166 @@
+/*
+ * zrk_oracle.h -- CPU ORACLE (test infrastructure only, never shipped).
+ *
+ * A plain-C restatement of Zero-RK's batched stiff-reactor hot path, used as
+ * the checker for the sm_100a kernels.  Only tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline leg load it.  Each function cites the reference
+ * file:line it restates (paths relative to the Zero-RK checkout).
+ *
+ * Parity pinning: the rate/thermo/RHS functions are checked against the
+ * reference's own zerork::mechanism library compiled from its sources by
+ * oracle/Makefile (oracle/_ref), and against the closed-form known-answer
+ * tests of tests/reactions/troe_gtest.cpp (6e-15 relative).
+ */
+#ifndef ZRK_ORACLE_H
+#define ZRK_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Falloff kinds: src/zerork/rate_const.h:13-16 (LINDEMANN, TROE_THREE_PARAMS,
+ * TROE_FOUR_PARAMS, SRI). */
+enum { ZO_FO_LINDEMANN = 0, ZO_FO_TROE3 = 1, ZO_FO_TROE4 = 2, ZO_FO_SRI = 3 };
+
+/* Mechanism tables in the reference's own indexing:
+ *  - species order = SPECIES section order (mechanism.cpp:117-138)
+ *  - step order    = fwd, rev interleaved per reaction (info_net.cpp:65-97)
+ *  - reactant/product lists expanded by integer stoichiometry
+ *    (info_net.cpp:219-330)
+ *  - Arrhenius parameters after unit conversion and the 1e-6 distinct-value
+ *    merge (rate_const.cpp:266-332, :1093-1106), listed per step
+ *  - reverse-from-Keq steps (rate_const.cpp:334-384)
+ *  - third-body and falloff lists (rate_const.cpp:386-537), efficiencies in
+ *    std::map (species-name) order, alpha = efficiency - 1.
+ * fo_par holds 8 doubles per falloff reaction:
+ *  [ln(Alow'), n_low, Ta_low, p3, p4, p5, p6, p7]
+ *  Troe: p3=alpha, p4=T***, p5=T*, p6=T** (Troe4 only)
+ *  SRI : p3=a, p4=b, p5=1/c (or -1), p6=d (1 if absent), p7=e (0 if absent) */
+typedef struct zo_tables {
+  int nsp, nrxn, nstep;
+  int tot_reac, tot_prod;
+  int n_arr, n_keq, n_tb, n_fo, n_tb_eff, n_fo_eff;
+  double *mw;        /* [nsp] kg/kmol */
+  double *thermo;    /* [nsp*16]: Tmid, 7 low, 7 high, pad */
+  int *step_rxn;     /* [nstep] */
+  int *step_dir;     /* [nstep] +1 fwd / -1 rev */
+  int *reac_ptr;     /* [nstep+1] */
+  int *reac_spc;     /* [tot_reac] */
+  int *prod_ptr;     /* [nstep+1] */
+  int *prod_spc;     /* [tot_prod] */
+  int *arr_step;     /* [n_arr] ascending step index */
+  double *arr_lnA, *arr_n, *arr_Ta;  /* [n_arr] */
+  int *keq_step, *keq_fwd;           /* [n_keq] */
+  double *keq_dn;                    /* [n_keq] nProd - nReac of fwd step */
+  int *tb_fwd, *tb_rev, *tb_ptr, *tb_spc;  /* rev = -1 if irreversible */
+  double *tb_alpha;
+  int *fo_fwd, *fo_rev, *fo_type, *fo_spc, *fo_ptr, *fo_eff_spc;  /* fo_spc=-1 => M */
+  double *fo_alpha, *fo_par;
+} zo_tables;
+
+zo_tables *zo_tables_alloc(const int sizes[11]); /* nsp,nrxn,nstep,tot_reac,tot_prod,
+                                                   n_arr,n_keq,n_tb,n_fo,n_tb_eff,n_fo_eff */
+void zo_tables_free(zo_tables *t);
+
+/* Physical constants: src/zerork/constants.h:10-24 */
+#define ZO_RU 8.314462618e3
+#define ZO_PATM 1.01325e5
+
+/* ---- thermo: src/zerork/nasa_poly.cpp:50-172 ---- */
+void zo_cp_R(const zo_tables *t, double T, double *cp_R);
+void zo_h_RT(const zo_tables *t, double T, double *h_RT);
+void zo_g_RT(const zo_tables *t, double T, double *g_RT);
+
+/* ---- rate coefficients: src/zerork/rate_const.cpp:539-582 (updateK) ---- */
+void zo_rate_coefs(const zo_tables *t, double T, const double *C, double *K);
+
+/* ---- rates: src/zerork/perf_net.cpp:190-274 (calcRatesFromTC_StepLimiter);
+ * lim may be NULL for perf_net.cpp:126-188 (calcRatesFromTC). ---- */
+void zo_rates(const zo_tables *t, double T, const double *C, const double *lim,
+              double *net, double *cre, double *des, double *rop);
+
+/* Kinetics provider: the reactor/Jacobian restatement calls mechanism-level
+ * functions through this table so the same assembly code can run on top of
+ * either this restatement or the reference library itself. */
+typedef struct zo_kinetics {
+  void *ctx;
+  void (*rates_limiter)(void *ctx, double T, const double *C, const double *lim,
+                        double *net, double *cre, double *des, double *rop);
+  void (*int_energy_RT)(void *ctx, double T, double *u_RT);
+  double (*mass_cv)(void *ctx, double T, const double *y, double *cv_spc);
+  double (*density_TPY)(void *ctx, double T, double P, const double *y);
+  void (*c_from_vy)(void *ctx, double v, const double *y, double *c);
+} zo_kinetics;
+
+void zo_kinetics_oracle(const zo_tables *t, zo_kinetics *k);
+
+/* Constant-volume reactor state (applications/cfd_plugin/
+ * reactor_constant_volume_cpu.cpp:15-41 InitializeState). */
+typedef struct zo_reactor {
+  const zo_tables *t;
+  zo_kinetics kin;
+  int nsp, nstep;
+  double inv_density, Tref, min_mass_frac;
+  double *lim, *C, *net, *cre, *des, *rop, *u_RT, *cv_spc, mean_cv;
+  double *tmp1, *tmp2, *tmp3;
+  double *yscale;  /* [nsp+1] rounding scale of the last ydot: sum of |terms| */
+  double *fscale;  /* [nsp+1] yscale of the caller's fy (set by the batch driver) */
+} zo_reactor;
+
+zo_reactor *zo_reactor_new(const zo_tables *t, const zo_kinetics *kin,
+                           double Tref, double min_mass_frac, double step_limiter);
+void zo_reactor_free(zo_reactor *r);
+/* Density from (T, P, Y): sets inv_density. */
+void zo_reactor_set_density(zo_reactor *r, double T, double P, const double *Y);
+
+/* ydot for y = [Y, T/Tref]: reactor_constant_volume_cpu.cpp:64-128.
+ * Returns 1 if T <= 0 (line 83). */
+int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot);
+
+/* Fixed Jacobian pattern: reactor_nvector_serial.cpp:122-281
+ * (SetupSparseJacobianArrays), CSC over n = nsp+1 variables. */
+typedef struct zo_jac_pattern {
+  int n, nnz;
+  int *col_ptr;   /* [n+1] */
+  int *row_idx;   /* [nnz] */
+  int *last_row;  /* [n]  index of row nsp in column j */
+  int n_des, n_cre;
+  int *des_conc, *des_step, *des_nz;  /* destruction terms */
+  int *cre_conc, *cre_step, *cre_nz;  /* creation terms */
+} zo_jac_pattern;
+
+zo_jac_pattern *zo_jac_pattern_new(const zo_tables *t);
+void zo_jac_pattern_free(zo_jac_pattern *p);
+
+/* Jacobian values at y (fy = ydot(y)): reactor_nvector_serial.cpp:610-771
+ * (SetupJacobianSparse).  If scale != NULL it receives, per nonzero, the sum
+ * of magnitudes of the analytic terms (the natural rounding-error scale). */
+int zo_jac_values(zo_reactor *r, const zo_jac_pattern *p, const double *y,
+                  const double *fy, double *jac, double *scale);
+
+/* Batched driver over independent (T, P, Y) states, reactor-major arrays.
+ * Per state: inverse density from (T,P,Y); y = [Y, T/Tref]; fy = ydot(y);
+ * wdot = net production rates at y; jac = Jacobian values at y.
+ * kins[nthreads]: one provider per thread (providers are not thread-safe). */
+int zo_batch_rates_jac(const zo_tables *t, const zo_jac_pattern *p,
+                       const zo_kinetics *kins, int nthreads,
+                       int nstates, const double *T, const double *P,
+                       const double *Y, double Tref, double min_mass_frac,
+                       double step_limiter, double *wdot, double *jac,
+                       double *ydot);
+
+/* As zo_batch_rates_jac, also returning rounding scales: wscale = create +
+ * destroy per species (the magnitude net = create - destroy cancels from),
+ * jscale = sum of magnitudes of the terms of each Jacobian entry (for the
+ * forward-difference column: the term magnitudes of both right-hand sides
+ * divided by the temperature step).  Serial. */
+int zo_batch_rates_jac_scaled(const zo_tables *t, const zo_jac_pattern *p,
+                              int nstates, const double *T, const double *P,
+                              const double *Y, double Tref, double min_mass_frac,
+                              double step_limiter, double *wdot, double *jac,
+                              double *wscale, double *jscale);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,148 @@
+"""Pin the CPU oracle (oracle/zrk_oracle.c) before trusting it.
+
+* against the reference's own zerork::mechanism library compiled from its
+  sources (oracle/_ref), on the reference's shipped mechanisms and on the
+  synthetic ones;
+* against the committed golden fixtures (reference outputs, tests/golden);
+* against the closed-form Troe known answers of the reference's
+  tests/reactions/troe_gtest.cpp (6e-15 relative there), restated here.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REF_DATA, golden, oracle_tables, ref_built, scaled_err
+
+import zrk_oracle as zo
+
+needs_ref = pytest.mark.skipif(not ref_built(), reason="oracle/_ref or reference data missing")
+
+
+def _conc(tables, T, P, Y):
+    mw = tables["mw"]
+    rho = P / (8.314462618e3 * T * np.sum(Y * (1.0 / mw)))
+    return (1.0 / (1.0 / rho)) * (1.0 / mw) * Y
+
+
+@needs_ref
+@pytest.mark.parametrize("mech,therm", [
+    ("hydrogen/h2_v1b_mech.txt", "hydrogen/h2_v1a_therm.txt"),
+    ("ideal/troe_test.mech", "ideal/const_specific_heat.therm"),
+    ("ideal/sri_reaction.mech", "ideal/const_specific_heat.therm"),
+    ("ideal/hydrogen_no_falloff.mech", "ideal/const_specific_heat.therm"),
+    ("dme/dme_24_mech.txt", "dme/dme_24_therm.txt"),
+])
+def test_oracle_matches_reference_library(mech, therm):
+    m, t = os.path.join(REF_DATA, mech), os.path.join(REF_DATA, therm)
+    if not (os.path.exists(m) and os.path.exists(t)):
+        pytest.skip("mechanism not shipped")
+    ref = zo.RefMechanism(m, t)
+    ot = zo.OracleTables(ref.tables)
+    rng = np.random.default_rng(0)
+    lim = np.full(ref.nstep, 1e22)
+    for _ in range(40):
+        T = rng.uniform(300, 3000)
+        C = rng.uniform(0, 1, ref.nsp) * 10 ** rng.uniform(-4, 1)
+        for a, b in zip(ref.rates(T, C, lim), ot.rates(T, C, lim)):
+            np.testing.assert_array_equal(a, b)  # same arithmetic, libc exp
+        for a, b in zip(ref.thermo(T), ot.thermo(T)):
+            np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+def test_oracle_batch_jacobian_on_reference_rates(tmp_path):
+    """The restated Jacobian assembly gives identical values whether it runs on
+    the oracle's rates or on the reference library's rates."""
+    from zerork_b200 import mechgen
+    g = mechgen.generate(mechgen.SPECS["c1_h2"])
+    m, t = g.write(str(tmp_path))
+    ref = zo.RefMechanism(m, t)
+    ot = zo.OracleTables(ref.tables)
+    T, P, Y = mechgen.rate_states(g, 64, seed=5)
+    w1, j1 = ref.batch_rates_jac((m, t), ot, T, P, Y, nthreads=2)
+    w2, j2, _ = ot.batch_rates_jac(T, P, Y, nthreads=2)
+    np.testing.assert_array_equal(w1, w2)
+    np.testing.assert_array_equal(j1, j2)
+
+
+@pytest.mark.parametrize("name", ["c1_h2", "c2_53"])
+def test_oracle_against_golden(name, mech_dir):
+    """Golden fixtures = reference-library outputs; regenerate with tests/golden/make_golden.py."""
+    import hashlib
+    from conftest import synth
+    g, (m, t) = synth(name, mech_dir)
+    gd = golden(name)
+    assert str(gd["text_hash"]) == hashlib.sha256((g.mech_text + g.therm_text).encode()).hexdigest()
+    import zerork_b200 as zb
+    pm = zb.Mechanism(m, t, device=False)
+    ot = oracle_tables(pm)
+    w, j, ws, js = ot.batch_rates_jac_scaled(gd["T"], gd["P"], gd["Y"])
+    assert scaled_err(w, gd["wdot"], ws) < 1e-13
+    assert scaled_err(j, gd["jac"], js) < 1e-12
+    for i in range(len(gd["T"])):
+        C = _conc(ot.d, gd["T"][i], gd["P"][i], gd["Y"][i])
+        net, cre, des, rop = ot.rates(gd["T"][i], C, np.full(ot.nstep, 1e22))
+        np.testing.assert_allclose(rop, gd["rop"][i], rtol=1e-14, atol=0)
+        np.testing.assert_allclose(cre, gd["cre"][i], rtol=1e-14, atol=0)
+
+
+TROE_MECH = """ELEMENTS
+H
+END
+SPECIES
+H H2
+END
+REACTIONS CAL/MOLE
+H2(+M) => H + H (+M)   2.0E12 0.0 0.0
+  LOW / 2.0E9 0.0 0.0 /
+  TROE / 0.68 78.0 1995.0 /
+H2(+M) => H + H (+M)   2.0E12 0.0 0.0
+  LOW / 2.0E9 0.0 0.0 /
+  TROE / 0.68 78.0 1995.0 5590.0 /
+END
+"""
+
+
+def _nasa_const_cp(name, comp, a0, a5, a6):
+    def e(v):
+        return f"{v:15.8E}"
+    l1 = f"{name:<16s}{'KA':<8s}{comp:<20s}G{300.0:10.2f}{5000.0:10.2f}{1000.0:8.2f}"
+    l1 = f"{l1:<79s}1"
+    l2 = e(a0) + e(0) * 4
+    l3 = e(a5) + e(a6) + e(a0) + e(0) * 2
+    l4 = e(0) * 2 + e(a5) + e(a6)
+    return [l1, f"{l2:<79s}2", f"{l3:<79s}3", f"{l4:<79s}4"]
+
+
+def test_troe_known_answer(tmp_path):
+    """Closed-form Troe falloff (3- and 4-parameter) as in the reference's
+    tests/reactions/troe_gtest.cpp: Khigh = 2e12 (1/s), Klow = 2e6 (m^3/kmol/s
+    after the mol/cm^3 -> kmol/m^3 conversion), alpha = 0.68, T*** = 78,
+    T* = 1995, T** = 5590, uniform composition at 1000 K and 1 atm."""
+    th = ["THERMO ALL", f"{300.0:10.3f}{1000.0:10.3f}{5000.0:10.3f}"]
+    th += _nasa_const_cp("H", "H   1", 2.5, 2.54737667e4, -4.46703359e-1)
+    th += _nasa_const_cp("H2", "H   2", 3.5, -1.043525e3, -4.22439182)
+    th.append("END")
+    (tmp_path / "t.mech").write_text(TROE_MECH)
+    (tmp_path / "t.therm").write_text("\n".join(th) + "\n")
+    import zerork_b200 as zb
+    pm = zb.Mechanism(str(tmp_path / "t.mech"), str(tmp_path / "t.therm"), device=False)
+    ot = oracle_tables(pm)
+    T, P = 1000.0, 1.01325e5
+    C = np.full(2, 0.5 * P / (8.314462618e3 * T))
+    K = ot.rate_coefs(T, C)
+    Csum = C.sum()
+    for rxn, four in ((0, False), (1, True)):
+        Pr = 2.0e6 * Csum / 2.0e12
+        Fc = (1 - 0.68) * math.exp(-T / 78.0) + 0.68 * math.exp(-T / 1995.0)
+        if four:
+            Fc += math.exp(-5590.0 / T)
+        f = math.log10(Fc)
+        n = 0.75 - 1.27 * f
+        lp = math.log10(Pr) - (0.4 + 0.67 * f)
+        lp = lp / (n - 0.14 * lp)
+        F = 10 ** (f / (1 + lp * lp))
+        expect = 2.0e12 * F * Pr / (1 + Pr)
+        assert abs(K[rxn] - expect) <= 6e-15 * abs(expect)

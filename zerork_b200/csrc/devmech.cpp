@@ -1,0 +1,166 @@
+// devmech.cpp -- pack MechTables + JacPattern into one device allocation.
+#include "devmech.h"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+namespace zrk {
+namespace {
+
+const double kRu = 8.314462618e3;
+
+struct Blob {
+  std::vector<unsigned char> bytes;
+  template <class T>
+  size_t add(const std::vector<T> &v) {
+    size_t off = (bytes.size() + 255) & ~size_t(255);
+    bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 16), 0);
+    if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+    return off;
+  }
+};
+
+void check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+}  // namespace
+
+DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
+  const int ns = t.nsp;
+  std::vector<double> inv_mw(ns), ru_inv_mw(ns);
+  for (int j = 0; j < ns; ++j) {
+    inv_mw[j] = 1.0 / t.mw[j];          // mechanism.cpp:135 invMolWt
+    ru_inv_mw[j] = kRu / t.mw[j];       // mechanism.cpp:136 RuInvMolWt
+  }
+  // reaction records
+  std::vector<RxnRec> rec(t.nrxn);
+  std::vector<int> arr_of_step(t.nstep, -1);
+  for (size_t k = 0; k < t.arr_step.size(); ++k) arr_of_step[t.arr_step[k]] = (int)k;
+  std::vector<int> step_of_fwd(t.nrxn, -1), step_of_rev(t.nrxn, -1);
+  for (int s = 0; s < t.nstep; ++s) {
+    if (t.step_dir[s] == 1) step_of_fwd[t.step_rxn[s]] = s;
+    else step_of_rev[t.step_rxn[s]] = s;
+  }
+  for (int j = 0; j < t.nrxn; ++j) {
+    RxnRec &R = rec[j];
+    std::memset(&R, 0, sizeof(R));
+    R.fwd = step_of_fwd[j];
+    R.rev = step_of_rev[j];
+    int a = arr_of_step[R.fwd];
+    if (a < 0) throw std::runtime_error("forward step without Arrhenius parameters");
+    R.lnA = t.arr_lnA[a];
+    R.n = t.arr_n[a];
+    R.Ta = t.arr_Ta[a];
+    if (R.rev >= 0) {
+      int b = arr_of_step[R.rev];
+      if (b >= 0) {
+        R.flags |= kRevArr;
+        R.lnA_r = t.arr_lnA[b];
+        R.n_r = t.arr_n[b];
+        R.Ta_r = t.arr_Ta[b];
+      } else {
+        R.flags |= kRevKeq;
+      }
+    }
+    R.nr = t.reac_ptr[R.fwd + 1] - t.reac_ptr[R.fwd];
+    R.np = t.prod_ptr[R.fwd + 1] - t.prod_ptr[R.fwd];
+    if (R.nr > kMaxSide || R.np > kMaxSide)
+      throw std::runtime_error("reaction " + std::to_string(j) + " has more than 6 species on a side");
+    for (int k = 0; k < R.nr; ++k) R.r[k] = (short)t.reac_spc[t.reac_ptr[R.fwd] + k];
+    for (int k = 0; k < R.np; ++k) R.p[k] = (short)t.prod_spc[t.prod_ptr[R.fwd] + k];
+    R.aux = -1;
+  }
+  for (size_t k = 0; k < t.keq_step.size(); ++k) {
+    int j = t.step_rxn[t.keq_fwd[k]];
+    rec[j].lnA_r = t.keq_dn[k];  // dn stored in the reverse slot
+  }
+  for (size_t k = 0; k < t.tb_fwd.size(); ++k) {
+    int j = t.step_rxn[t.tb_fwd[k]];
+    rec[j].flags |= kThirdBody;
+    rec[j].aux = (int)k;
+  }
+  for (size_t k = 0; k < t.fo_fwd.size(); ++k) {
+    int j = t.step_rxn[t.fo_fwd[k]];
+    rec[j].flags |= kFalloff;
+    rec[j].aux = (int)k;
+  }
+  // species gather lists, ascending step order (perf_net.cpp:257-267 sum order)
+  std::vector<std::vector<int>> sd(ns), sc(ns);
+  for (int s = 0; s < t.nstep; ++s) {
+    for (int k = t.reac_ptr[s]; k < t.reac_ptr[s + 1]; ++k) sd[t.reac_spc[k]].push_back(s);
+    for (int k = t.prod_ptr[s]; k < t.prod_ptr[s + 1]; ++k) sc[t.prod_spc[k]].push_back(s);
+  }
+  std::vector<int> sd_ptr(1, 0), sd_step, sc_ptr(1, 0), sc_step;
+  for (int j = 0; j < ns; ++j) {
+    sd_step.insert(sd_step.end(), sd[j].begin(), sd[j].end());
+    sd_ptr.push_back((int)sd_step.size());
+    sc_step.insert(sc_step.end(), sc[j].begin(), sc[j].end());
+    sc_ptr.push_back((int)sc_step.size());
+  }
+  // Jacobian per-nonzero gather lists, in term-list order
+  // (reactor_nvector_serial.cpp:659-673: all destruction terms, then creation)
+  std::vector<std::vector<int>> nzd(p.nnz), nzc(p.nnz);
+  for (size_t q = 0; q < p.des_nz.size(); ++q) nzd[p.des_nz[q]].push_back(p.des_step[q]);
+  for (size_t q = 0; q < p.cre_nz.size(); ++q) nzc[p.cre_nz[q]].push_back(p.cre_step[q]);
+  std::vector<int> nzd_ptr(1, 0), nzd_step, nzc_ptr(1, 0), nzc_step;
+  for (int k = 0; k < p.nnz; ++k) {
+    nzd_step.insert(nzd_step.end(), nzd[k].begin(), nzd[k].end());
+    nzd_ptr.push_back((int)nzd_step.size());
+    nzc_step.insert(nzc_step.end(), nzc[k].begin(), nzc[k].end());
+    nzc_ptr.push_back((int)nzc_step.size());
+  }
+  n_terms_ = (int)(nzd_step.size() + nzc_step.size());
+
+  Blob b;
+  size_t o_mw = b.add(t.mw), o_imw = b.add(inv_mw), o_rimw = b.add(ru_inv_mw), o_th = b.add(t.thermo);
+  size_t o_rec = b.add(rec);
+  size_t o_tbp = b.add(t.tb_ptr), o_tbs = b.add(t.tb_spc), o_tba = b.add(t.tb_alpha);
+  size_t o_fop = b.add(t.fo_ptr), o_foe = b.add(t.fo_eff_spc), o_fot = b.add(t.fo_type),
+         o_fos = b.add(t.fo_spc), o_foa = b.add(t.fo_alpha), o_fopar = b.add(t.fo_par);
+  size_t o_sdp = b.add(sd_ptr), o_sds = b.add(sd_step), o_scp = b.add(sc_ptr), o_scs = b.add(sc_step);
+  size_t o_cp = b.add(p.col_ptr), o_ri = b.add(p.row_idx), o_lr = b.add(p.last_row);
+  size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
+  bytes_ = b.bytes.size();
+  check(cudaMalloc(&blob_, bytes_), "cudaMalloc(mechanism tables)");
+  check(cudaMemcpy(blob_, b.bytes.data(), bytes_, cudaMemcpyHostToDevice), "cudaMemcpy(mechanism tables)");
+  auto P = [&](size_t off) { return (const void *)((const unsigned char *)blob_ + off); };
+  view_.nsp = ns;
+  view_.nrxn = t.nrxn;
+  view_.nstep = t.nstep;
+  view_.nnz = p.nnz;
+  view_.mw = (const double *)P(o_mw);
+  view_.inv_mw = (const double *)P(o_imw);
+  view_.ru_inv_mw = (const double *)P(o_rimw);
+  view_.thermo = (const double *)P(o_th);
+  view_.rxn = (const RxnRec *)P(o_rec);
+  view_.tb_ptr = (const int *)P(o_tbp);
+  view_.tb_spc = (const int *)P(o_tbs);
+  view_.tb_alpha = (const double *)P(o_tba);
+  view_.fo_ptr = (const int *)P(o_fop);
+  view_.fo_spc_eff = (const int *)P(o_foe);
+  view_.fo_type = (const int *)P(o_fot);
+  view_.fo_spc = (const int *)P(o_fos);
+  view_.fo_alpha = (const double *)P(o_foa);
+  view_.fo_par = (const double *)P(o_fopar);
+  view_.sd_ptr = (const int *)P(o_sdp);
+  view_.sd_step = (const int *)P(o_sds);
+  view_.sc_ptr = (const int *)P(o_scp);
+  view_.sc_step = (const int *)P(o_scs);
+  view_.col_ptr = (const int *)P(o_cp);
+  view_.row_idx = (const int *)P(o_ri);
+  view_.last_row = (const int *)P(o_lr);
+  view_.nzd_ptr = (const int *)P(o_ndp);
+  view_.nzd_step = (const int *)P(o_nds);
+  view_.nzc_ptr = (const int *)P(o_ncp);
+  view_.nzc_step = (const int *)P(o_ncs);
+}
+
+DeviceMechanism::~DeviceMechanism() {
+  if (blob_) cudaFree(blob_);
+}
+
+}  // namespace zrk

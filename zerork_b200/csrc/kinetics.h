@@ -1,0 +1,43 @@
+// kinetics.h -- launchers for the fused FP64 rates + Jacobian kernel.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+#include "devmech.h"
+
+namespace zrk {
+
+struct KinParams {
+  double Tref;     // reference_temperature option (state y[S] = T / Tref)
+  double mmf;      // min_mass_fraction option (Jacobian clamp)
+  double lim;      // step_limiter option (same value for every step)
+  double sqrt_ur;  // sqrt(DBL_EPSILON), the forward-difference scale
+};
+
+// Tile / CTA mapping: ts states per tile (8, 16 or 32), warps per CTA, and
+// whether the per-tile workspace lives in global scratch (grid CTAs, each
+// with its own slice) instead of shared memory.
+struct LaunchCfg {
+  int ts = 16;
+  int warps = 8;
+  bool global_ws = false;
+  int grid = 0;
+};
+
+// Species-major arrays x[item * ld + state]; ld >= n.
+struct RatesJacArgs {
+  int n = 0, ld = 0;
+  const double *T = nullptr, *P = nullptr, *Y = nullptr;  // Y: [nsp][ld]
+  double *wdot = nullptr;                                 // [nsp][ld]  (required)
+  double *jac = nullptr;                                  // [nnz][ld]  (optional)
+  double *ydot = nullptr;                                 // [nsp+1][ld] (optional)
+  double *scratch = nullptr;                              // global workspace
+  size_t scratch_bytes = 0;
+};
+
+size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg);
+cudaError_t launch_rates_jac(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
+                             const LaunchCfg &cfg, cudaStream_t stream);
+
+}  // namespace zrk
