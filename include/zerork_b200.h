@@ -69,11 +69,20 @@ int zrk_mech_jac_pattern(zrk_mech_t m, int *col_ptr, int *row_idx);
 int zrk_mech_set_double_option(zrk_mech_t m, const char *name, double value);
 int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value);
 
-/* Tile mapping of the rate kernel: ts states per tile (8/16/32), warps per
- * CTA (1..16), global_ws = 1 puts the per-tile workspace in global scratch
- * (grid CTAs; 0 = one CTA per tile).  ts = 0 selects the autotuned mapping. */
-int zrk_mech_set_launch(zrk_mech_t m, int ts, int warps, int global_ws, int grid);
-int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *warps, int *global_ws, int *grid);
+/* Tile mapping of the rate kernel: ts states per tile (8/16/32), v states
+ * per thread (1/2/4), warps per CTA (1..16), global_ws = 1 puts the per-tile
+ * workspace in global scratch (grid CTAs; 0 = one CTA per tile).  ts = 0
+ * restores the default mapping. */
+int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int global_ws, int grid);
+int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *global_ws, int *grid);
+
+/* Autotuner: times every valid (ts, v, warps) mapping on the caller's sample
+ * (device arrays as for zrk_rates_jac_dev, outputs overwritten) and keeps the
+ * fastest for later calls.  *best_ms (may be NULL) receives its time.  No
+ * counterpart in the reference, whose launch shapes are fixed constants
+ * (src/zerork/rate_const_cuda.cpp:583-629, "tuned on P100"). */
+int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double *P,
+                      const double *Y, double *wdot, double *jac, void *stream, float *best_ms);
 
 /* Net production rates + reactor Jacobian at independent (T, P, Y) states,
  * all device pointers on the current device, species-major with leading

@@ -44,8 +44,10 @@ def lib():
         L.zrk_mech_jac_pattern.argtypes = [vp, vp, vp]
         L.zrk_mech_set_double_option.argtypes = [vp, C.c_char_p, C.c_double]
         L.zrk_mech_get_double_option.argtypes = [vp, C.c_char_p, dp]
-        L.zrk_mech_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
-        L.zrk_mech_get_launch.argtypes = [vp, ip, ip, ip, ip]
+        L.zrk_mech_set_launch.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.zrk_mech_get_launch.argtypes = [vp, ip, ip, ip, ip, ip]
+        L.zrk_mech_autotune.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp,
+                                        C.POINTER(C.c_float)]
         L.zrk_rates_jac_dev.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp]
         L.zrk_rates_jac_host.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
         L.zrk_measure_fp64.argtypes = [dp, dp]
@@ -143,13 +145,24 @@ class Mechanism:
         check(lib().zrk_mech_get_double_option(self._h, name.encode(), C.byref(v)))
         return v.value
 
-    def set_launch(self, ts=0, warps=8, global_ws=False, grid=0):
-        check(lib().zrk_mech_set_launch(self._h, ts, warps, 1 if global_ws else 0, grid))
+    def set_launch(self, ts=0, v=1, warps=8, global_ws=False, grid=0):
+        check(lib().zrk_mech_set_launch(self._h, ts, v, warps, 1 if global_ws else 0, grid))
 
     def get_launch(self):
-        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        check(lib().zrk_mech_get_launch(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)))
-        return dict(ts=a.value, warps=b.value, global_ws=bool(c.value), grid=d.value)
+        a, b, c, d, e = C.c_int(), C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        check(lib().zrk_mech_get_launch(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d),
+                                        C.byref(e)))
+        return dict(ts=a.value, v=b.value, warps=c.value, global_ws=bool(d.value), grid=e.value)
+
+    def autotune(self, T, P, Y, wdot, jac=None, n=None, stream=None):
+        """Time every tile/warp mapping on a device sample; keep the fastest."""
+        ld = Y.shape[1]
+        n = ld if n is None else n
+        s = None if stream is None else C.c_void_p(stream)
+        ms = C.c_float()
+        check(lib().zrk_mech_autotune(self._h, n, ld, _ptr(T), _ptr(P), _ptr(Y), _ptr(wdot),
+                                      _ptr(jac), s, C.byref(ms)))
+        return self.get_launch(), ms.value
 
     def rates_jac(self, T, P, Y, wdot, jac=None, ydot=None, n=None, stream=None):
         """Device tensors, species-major: Y[nsp, ld], wdot[nsp, ld], jac[nnz, ld]."""

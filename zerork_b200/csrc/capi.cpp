@@ -27,16 +27,19 @@ int cuda_error(cudaError_t e, const char *what) {
 }
 
 LaunchCfg default_launch(const DevMech &m) {
-  // Largest tile whose workspace fits in shared memory at 8 warps per CTA.
+  // Largest tile whose workspace fits in shared memory at 8 warps per CTA,
+  // two states per thread; the autotuner (zrk_mech_autotune) refines this.
   const size_t kMaxSmem = 227 * 1024;
   for (int ts : {16, 8}) {
     LaunchCfg c;
     c.ts = ts;
+    c.v = 2;
     c.warps = 8;
     if (rates_jac_ws_bytes(m, c) <= kMaxSmem) return c;
   }
   LaunchCfg c;
   c.ts = 16;
+  c.v = 2;
   c.warps = 8;
   c.global_ws = true;
   int dev = 0, sms = 148;
@@ -205,7 +208,7 @@ int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value) {
   return ZRK_OK;
 }
 
-int zrk_mech_set_launch(zrk_mech_t m, int ts, int warps, int global_ws, int grid) {
+int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int global_ws, int grid) {
   if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
   MechHandle *h = reinterpret_cast<MechHandle *>(m);
   if (!h->dev) return set_error(ZRK_ERR_NO_DEVICE, "handle has no device tables (zrk_mech_parse)");
@@ -213,26 +216,79 @@ int zrk_mech_set_launch(zrk_mech_t m, int ts, int warps, int global_ws, int grid
     h->cfg = default_launch(h->dev->view());
     return ZRK_OK;
   }
-  if (!(ts == 8 || ts == 16 || ts == 32) || warps < 1 || warps > 16 || grid < 0)
-    return set_error(ZRK_ERR_INVALID_ARGUMENT, "bad launch mapping");
   LaunchCfg c;
   c.ts = ts;
+  c.v = v;
   c.warps = warps;
   c.global_ws = global_ws != 0;
   c.grid = grid;
+  if (!rates_jac_mapping_ok(c) || grid < 0)
+    return set_error(ZRK_ERR_INVALID_ARGUMENT, "bad launch mapping");
   if (!c.global_ws && rates_jac_ws_bytes(h->dev->view(), c) > 227 * 1024)
     return set_error(ZRK_ERR_INVALID_ARGUMENT, "workspace does not fit in shared memory");
   h->cfg = c;
   return ZRK_OK;
 }
 
-int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *warps, int *global_ws, int *grid) {
+int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *global_ws, int *grid) {
   if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
   MechHandle *h = reinterpret_cast<MechHandle *>(m);
   if (ts) *ts = h->cfg.ts;
+  if (v) *v = h->cfg.v;
   if (warps) *warps = h->cfg.warps;
   if (global_ws) *global_ws = h->cfg.global_ws ? 1 : 0;
   if (grid) *grid = h->cfg.grid;
+  return ZRK_OK;
+}
+
+int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double *P,
+                      const double *Y, double *wdot, double *jac, void *stream, float *best_ms) {
+  if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
+  MechHandle *h = reinterpret_cast<MechHandle *>(m);
+  if (!h->dev) return set_error(ZRK_ERR_NO_DEVICE, "handle has no device tables (zrk_mech_parse)");
+  if (n <= 0 || ld < n || !T || !P || !Y || !wdot) return set_error(ZRK_ERR_INVALID_ARGUMENT, "bad sample");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  LaunchCfg best = h->cfg;
+  float best_t = 1e30f;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  for (int ts : {8, 16, 32})
+    for (int v : {1, 2, 4})
+      for (int warps : {4, 8, 16}) {
+        LaunchCfg c;
+        c.ts = ts;
+        c.v = v;
+        c.warps = warps;
+        if (!rates_jac_mapping_ok(c)) continue;
+        if (rates_jac_ws_bytes(h->dev->view(), c) > 227 * 1024) {
+          c.global_ws = true;
+          c.grid = 2 * sms;
+        }
+        h->cfg = c;
+        float t = 0.f;
+        bool ok = true;
+        for (int rep = 0; rep < 3 && ok; ++rep) {
+          cudaEventRecord(e0, st);
+          ok = zrk_rates_jac_dev(m, n, ld, T, P, Y, wdot, jac, nullptr, stream) == ZRK_OK;
+          cudaEventRecord(e1, st);
+          cudaEventSynchronize(e1);
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (rep > 0) t += ms;  // first launch warms up
+        }
+        if (ok && cudaGetLastError() == cudaSuccess && t < best_t) {
+          best_t = t;
+          best = c;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->cfg = best;
+  if (best_ms) *best_ms = best_t / 2;
   return ZRK_OK;
 }
 

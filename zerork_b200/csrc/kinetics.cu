@@ -42,6 +42,7 @@ struct Layout {
   int rC, rU, rX, rG, rROP, rPart, rScal, rows;
 };
 
+// NG here is the number of warps: one partial-sum row pair per warp.
 __host__ __device__ inline Layout make_layout(int S, int N, int NG) {
   Layout L;
   L.rC = 0;
@@ -50,7 +51,7 @@ __host__ __device__ inline Layout make_layout(int S, int N, int NG) {
   L.rG = 3 * S;
   L.rROP = 4 * S;
   L.rPart = 4 * S + N;
-  L.rScal = L.rPart + 3 * NG;
+  L.rScal = L.rPart + 2 * NG;
   L.rows = L.rScal + kNScal;
   return L;
 }
@@ -82,83 +83,134 @@ __device__ __forceinline__ double nasa_cp(const double *__restrict__ c, double T
   return c[o] + T * (c[o + 1] + T * (c[o + 2] + T * (c[o + 3] + T * c[o + 4])));
 }
 
-// One reaction (both steps) for one state: rate constants, third body,
-// falloff, step limiter and concentration products.
-template <int TS>
-__device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R, int sl,
+// One reaction (both steps) for the V states a thread owns (states
+// q + k*GS of the tile): rate constants, third body, falloff, step limiter
+// and concentration products.  The V independent chains give the scheduler
+// instruction-level parallelism across states.
+template <int TS, int V>
+__device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R, int q,
                                               const double *__restrict__ sC,
                                               const double *__restrict__ sG, double *sROP,
-                                              double T, double logT, double invT, double lprt,
-                                              double Csum, double lim) {
-  double kf = exp(R.lnA + R.n * logT - R.Ta * invT);
-  double kr = 0.0;
+                                              const double *T, const double *logT,
+                                              const double *invT, const double *lprt,
+                                              const double *Csum, double lim) {
+  constexpr int GS = TS / V;
+  double kf[V], kr[V];
+#pragma unroll
+  for (int k = 0; k < V; ++k) kf[k] = exp(R.lnA + R.n * logT[k] - R.Ta * invT[k]);
   if (R.flags & kRevArr) {
-    kr = exp(R.lnA_r + R.n_r * logT - R.Ta_r * invT);
+#pragma unroll
+    for (int k = 0; k < V; ++k) kr[k] = exp(R.lnA_r + R.n_r * logT[k] - R.Ta_r * invT[k]);
   } else if (R.flags & kRevKeq) {
-    double s = 0.0;
-    for (int k = 0; k < R.np; ++k) s += sG[R.p[k] * TS + sl];
-    for (int k = 0; k < R.nr; ++k) s -= sG[R.r[k] * TS + sl];
-    kr = exp(s - R.lnA_r * lprt) * kf;
+    double s[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) s[k] = 0.0;
+    for (int i = 0; i < R.np; ++i) {
+      const double *gp = sG + R.p[i] * TS + q;
+#pragma unroll
+      for (int k = 0; k < V; ++k) s[k] += gp[k * GS];
+    }
+    for (int i = 0; i < R.nr; ++i) {
+      const double *gr = sG + R.r[i] * TS + q;
+#pragma unroll
+      for (int k = 0; k < V; ++k) s[k] -= gr[k * GS];
+    }
+#pragma unroll
+    for (int k = 0; k < V; ++k) kr[k] = exp(s[k] - R.lnA_r * lprt[k]) * kf[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; ++k) kr[k] = 0.0;
   }
   if (R.flags & kThirdBody) {
-    double Cm = Csum;
-    for (int e = m.tb_ptr[R.aux]; e < m.tb_ptr[R.aux + 1]; ++e)
-      Cm += sC[m.tb_spc[e] * TS + sl] * m.tb_alpha[e];
-    kf *= Cm;
-    kr *= Cm;
+    double Cm[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
+    for (int e = m.tb_ptr[R.aux]; e < m.tb_ptr[R.aux + 1]; ++e) {
+      const double a = m.tb_alpha[e];
+      const double *cp = sC + m.tb_spc[e] * TS + q;
+#pragma unroll
+      for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
+    }
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      kf[k] *= Cm[k];
+      kr[k] *= Cm[k];
+    }
   }
   if (R.flags & kFalloff) {
     const int f = R.aux;
     const double *p = m.fo_par + 8 * f;
-    const double Klow = exp(p[0] + p[1] * logT - p[2] * invT);
-    double Cm;
     const int fs = m.fo_spc[f];
-    if (fs >= 0) {
-      Cm = sC[fs * TS + sl];
-    } else {
-      Cm = Csum;
-      for (int e = m.fo_ptr[f]; e < m.fo_ptr[f + 1]; ++e)
-        Cm += sC[m.fo_spc_eff[e] * TS + sl] * m.fo_alpha[e];
-    }
-    double Pr = Klow * Cm / kf;
-    if (Pr < 1.0e-300) Pr = 1.0e-300;
-    double lPr = log10(Pr);
-    double fT = 1.0;
     const int ty = m.fo_type[f];
-    if (ty == kTroe3 || ty == kTroe4) {
-      double Fc = 0.0;
-      if (p[4] != 0) Fc += (1.0 - p[3]) * exp(-T / p[4]);
-      if (p[5] != 0) Fc += p[3] * exp(-T / p[5]);
-      if (ty == kTroe4) Fc += exp(-p[6] * invT);
-      if (Fc < 1.0e-300) Fc = 1.0e-300;
-      fT = log10(Fc);
-      const double nT = 0.75 - 1.27 * fT;
-      lPr -= (0.4 + 0.67 * fT);
-      lPr = lPr / (nT - 0.14 * lPr);
-      lPr *= lPr;
-      fT /= (1.0 + lPr);
-      fT = pow(10.0, fT);
-    } else if (ty == kSRI) {
-      const double xp = 1.0 / (1.0 + lPr * lPr);
-      fT = p[3] * exp(-p[4] * invT);
-      if (p[5] > 0) fT += exp(-T * p[5]);
-      fT = pow(fT, xp);
-      fT *= p[6];
-      fT *= pow(T, p[7]);
+    double Cm[V];
+    if (fs >= 0) {
+#pragma unroll
+      for (int k = 0; k < V; ++k) Cm[k] = sC[fs * TS + q + k * GS];
+    } else {
+#pragma unroll
+      for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
+      for (int e = m.fo_ptr[f]; e < m.fo_ptr[f + 1]; ++e) {
+        const double a = m.fo_alpha[e];
+        const double *cp = sC + m.fo_spc_eff[e] * TS + q;
+#pragma unroll
+        for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
+      }
     }
-    const double Pc = fT * Pr / (1.0 + Pr);
-    kf *= Pc;
-    kr *= Pc;
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      const double Klow = exp(p[0] + p[1] * logT[k] - p[2] * invT[k]);
+      double Pr = Klow * Cm[k] / kf[k];
+      if (Pr < 1.0e-300) Pr = 1.0e-300;
+      double lPr = log10(Pr);
+      double fT = 1.0;
+      if (ty == kTroe3 || ty == kTroe4) {
+        double Fc = 0.0;
+        if (p[4] != 0) Fc += (1.0 - p[3]) * exp(-T[k] / p[4]);
+        if (p[5] != 0) Fc += p[3] * exp(-T[k] / p[5]);
+        if (ty == kTroe4) Fc += exp(-p[6] * invT[k]);
+        if (Fc < 1.0e-300) Fc = 1.0e-300;
+        fT = log10(Fc);
+        const double nT = 0.75 - 1.27 * fT;
+        lPr -= (0.4 + 0.67 * fT);
+        lPr = lPr / (nT - 0.14 * lPr);
+        lPr *= lPr;
+        fT /= (1.0 + lPr);
+        fT = pow(10.0, fT);
+      } else if (ty == kSRI) {
+        const double xp = 1.0 / (1.0 + lPr * lPr);
+        fT = p[3] * exp(-p[4] * invT[k]);
+        if (p[5] > 0) fT += exp(-T[k] * p[5]);
+        fT = pow(fT, xp);
+        fT *= p[6];
+        fT *= pow(T[k], p[7]);
+      }
+      const double Pc = fT * Pr / (1.0 + Pr);
+      kf[k] *= Pc;
+      kr[k] *= Pc;
+    }
   }
   if (0.0 < lim && lim < 1.0e300) {
-    kf *= lim / (lim + kf);
-    if (R.rev >= 0) kr *= lim / (lim + kr);
+#pragma unroll
+    for (int k = 0; k < V; ++k) {
+      kf[k] *= lim / (lim + kf[k]);
+      if (R.rev >= 0) kr[k] *= lim / (lim + kr[k]);
+    }
   }
-  for (int k = 0; k < R.nr; ++k) kf *= sC[R.r[k] * TS + sl];
-  sROP[R.fwd * TS + sl] = kf;
+  for (int i = 0; i < R.nr; ++i) {
+    const double *cp = sC + R.r[i] * TS + q;
+#pragma unroll
+    for (int k = 0; k < V; ++k) kf[k] *= cp[k * GS];
+  }
+#pragma unroll
+  for (int k = 0; k < V; ++k) sROP[R.fwd * TS + q + k * GS] = kf[k];
   if (R.rev >= 0) {
-    for (int k = 0; k < R.np; ++k) kr *= sC[R.p[k] * TS + sl];
-    sROP[R.rev * TS + sl] = kr;
+    for (int i = 0; i < R.np; ++i) {
+      const double *cp = sC + R.p[i] * TS + q;
+#pragma unroll
+      for (int k = 0; k < V; ++k) kr[k] *= cp[k * GS];
+    }
+#pragma unroll
+    for (int k = 0; k < V; ++k) sROP[R.rev * TS + q + k * GS] = kr[k];
   }
 }
 
@@ -167,322 +219,469 @@ __device__ __forceinline__ double clampy(double y, double mmf) {
   return y;
 }
 
-template <int TS>
-__global__ void __launch_bounds__(512, 1) rates_jac_kernel(
+// Sum over the groups of a warp (lanes q, q+GS, ...) with shuffles; lanes
+// q < GS of each warp then hold the warp's partial for their states.
+template <int GS>
+__device__ __forceinline__ double warp_group_sum(double v) {
+#pragma unroll
+  for (int o = GS; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Gather-sum of rates of progress over an index list, V states.
+template <int TS, int V>
+__device__ __forceinline__ void gather_rop(const double *__restrict__ sROP, const int *__restrict__ list,
+                                           int b, int e, int q, double *acc) {
+  constexpr int GS = TS / V;
+  for (int i = b; i < e; ++i) {
+    const double *rp = sROP + list[i] * TS + q;
+#pragma unroll
+    for (int k = 0; k < V; ++k) acc[k] += rp[k * GS];
+  }
+}
+
+template <int TS, int V, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     DevMech m, int n, int ld, const double *__restrict__ Tin, const double *__restrict__ Pin,
     const double *__restrict__ Y, double *__restrict__ wdot, double *__restrict__ jac,
     double *__restrict__ ydot, KinParams kp, double *__restrict__ gscratch, int ws_doubles) {
+  constexpr int GS = TS / V;
   extern __shared__ double smem_dyn[];
   const int S = m.nsp, N = m.nstep;
-  const int NG = blockDim.x / TS;
-  const int g = threadIdx.x / TS;
-  const int sl = threadIdx.x % TS;
-  const Layout L = make_layout(S, N, NG);
+  const int NW = blockDim.x >> 5;
+  const int NG = blockDim.x / GS;
+  const int g = threadIdx.x / GS;
+  const int q = threadIdx.x % GS;
+  const int w = threadIdx.x >> 5;
+  const bool wlead = (threadIdx.x & 31) < GS;  // holds the warp partial
+  const Layout L = make_layout(S, N, NW);
   double *ws = gscratch ? gscratch + (size_t)blockIdx.x * ws_doubles : smem_dyn;
   double *sC = ws + L.rC * TS, *sU = ws + L.rU * TS, *sX = ws + L.rX * TS, *sG = ws + L.rG * TS;
   double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS, *sc = ws + L.rScal * TS;
-#define SCAL(k) sc[(k) * TS + sl]
-#define PART(a, grp) sPart[((a) * NG + (grp)) * TS + sl]
+#define SC(r, k) sc[(r) * TS + q + (k) * GS]
+#define PT(a, ww, k) sPart[((a) * NW + (ww)) * TS + q + (k) * GS]
+#define FORV _Pragma("unroll") for (int k = 0; k < V; ++k)
   const int ntiles = (n + TS - 1) / TS;
   const double dummy_y = 1.0 / S;
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int st = tile * TS + sl;
-    const bool valid = st < n;
-    // ---- per-state inputs and mixture molecular weight
-    double pa = 0.0;
-    for (int s = g; s < S; s += NG) {
-      const double y = valid ? Y[(size_t)s * ld + st] : dummy_y;
-      pa += y * m.inv_mw[s];
+    int st[V];
+    bool valid[V];
+    FORV {
+      st[k] = tile * TS + q + k * GS;
+      valid[k] = st[k] < n;
     }
-    PART(0, g) = pa;
-    if (g == 0) {
-      const double T = valid ? Tin[st] : 1000.0;
-      const double P = valid ? Pin[st] : kPatm;
-      SCAL(S_T) = T;
-      SCAL(S_P) = P;
-      SCAL(S_YS) = T / kp.Tref;
-    }
-    __syncthreads();
-    if (g == 0) {
-      double sum = 0.0;
-      for (int q = 0; q < NG; ++q) sum += PART(0, q);
-      const double T = SCAL(S_T);
-      const double mwmix = 1.0 / sum;
-      const double rho = SCAL(S_P) * mwmix / (kRu * T);
-      SCAL(S_V) = 1.0 / rho;
-      double Tr = SCAL(S_YS) * kp.Tref;
-      if (Tr > 1.0e4) Tr = 1.0e4;
-      SCAL(S_TR) = Tr;
-      SCAL(S_LOGT) = log(Tr);
-      SCAL(S_INVT) = 1.0 / Tr;
-      SCAL(S_LPRT) = log(kPatm / (kRu * Tr));
-    }
-    __syncthreads();
-    // ---- species pass at T: C, g/RT, u/RT, partial sums
+    auto yload = [&](int s, int k) -> double {
+      return valid[k] ? Y[(size_t)s * ld + st[k]] : dummy_y;
+    };
+    // ---- mixture molecular weight partials
     {
-      const double v = SCAL(S_V), dens = 1.0 / v, Tr = SCAL(S_TR), logT = SCAL(S_LOGT);
-      double pc = 0.0, pcv = 0.0;
-      int need = 0;
+      double pa[V];
+      FORV pa[k] = 0.0;
       for (int s = g; s < S; s += NG) {
-        const double y = valid ? Y[(size_t)s * ld + st] : dummy_y;
-        const double c = dens * m.inv_mw[s] * y;
-        sC[s * TS + sl] = c;
-        double cp, h, gg;
-        nasa_cp_h_g(m.thermo + 16 * s, Tr, logT, &cp, &h, &gg);
-        sG[s * TS + sl] = gg;
-        sU[s * TS + sl] = h - 1.0;
-        const double cvs = (cp - 1.0) * m.ru_inv_mw[s];
-        pc += c;
-        pcv += cvs * y;
-        need |= (fabs(y) < kp.mmf);
+        const double iw = m.inv_mw[s];
+        FORV pa[k] += yload(s, k) * iw;
       }
-      PART(0, g) = pc;
-      PART(1, g) = pcv;
-      need = __syncthreads_or(need);
-      if (g == 0) {
+      FORV pa[k] = warp_group_sum<GS>(pa[k]);
+      if (wlead) FORV PT(0, w, k) = pa[k];
+    }
+    __syncthreads();
+    if (g == 0) {
+      FORV {
+        double sum = 0.0;
+        for (int ww = 0; ww < NW; ++ww) sum += PT(0, ww, k);
+        const double T = valid[k] ? Tin[st[k]] : 1000.0;
+        const double P = valid[k] ? Pin[st[k]] : kPatm;
+        const double yS = T / kp.Tref;
+        const double mwmix = 1.0 / sum;
+        const double rho = P * mwmix / (kRu * T);
+        SC(S_YS, k) = yS;
+        SC(S_V, k) = 1.0 / rho;
+        double Tr = yS * kp.Tref;
+        if (Tr > 1.0e4) Tr = 1.0e4;
+        SC(S_TR, k) = Tr;
+        SC(S_LOGT, k) = log(Tr);
+        SC(S_INVT, k) = 1.0 / Tr;
+        SC(S_LPRT, k) = log(kPatm / (kRu * Tr));
+      }
+    }
+    __syncthreads();
+    double v[V], Tr[V], logT[V], invT[V], lprt[V], Csum[V];
+    FORV {
+      v[k] = SC(S_V, k);
+      Tr[k] = SC(S_TR, k);
+      logT[k] = SC(S_LOGT, k);
+      invT[k] = SC(S_INVT, k);
+      lprt[k] = SC(S_LPRT, k);
+    }
+    // ---- species pass at T: C, g/RT, u/RT, partial sums
+    int need = 0;
+    {
+      double pc[V], pcv[V];
+      FORV pc[k] = pcv[k] = 0.0;
+      for (int s = g; s < S; s += NG) {
+        const double *th = m.thermo + 16 * s;
+        const double iw = m.inv_mw[s], riw = m.ru_inv_mw[s];
+        FORV {
+          const double y = yload(s, k);
+          const double c = (1.0 / v[k]) * iw * y;
+          sC[s * TS + q + k * GS] = c;
+          double cp, h, gg;
+          nasa_cp_h_g(th, Tr[k], logT[k], &cp, &h, &gg);
+          sG[s * TS + q + k * GS] = gg;
+          sU[s * TS + q + k * GS] = h - 1.0;
+          pc[k] += c;
+          pcv[k] += ((cp - 1.0) * riw) * y;
+          need |= (fabs(y) < kp.mmf);
+        }
+      }
+      FORV {
+        pc[k] = warp_group_sum<GS>(pc[k]);
+        pcv[k] = warp_group_sum<GS>(pcv[k]);
+      }
+      if (wlead) FORV {
+        PT(0, w, k) = pc[k];
+        PT(1, w, k) = pcv[k];
+      }
+    }
+    need = __syncthreads_or(need);
+    if (g == 0) {
+      FORV {
         double cs = 0.0, cv = 0.0;
-        for (int q = 0; q < NG; ++q) {
-          cs += PART(0, q);
-          cv += PART(1, q);
+        for (int ww = 0; ww < NW; ++ww) {
+          cs += PT(0, ww, k);
+          cv += PT(1, ww, k);
         }
-        SCAL(S_CSUM) = cs;
-        SCAL(S_CV) = cv;
+        SC(S_CSUM, k) = cs;
+        SC(S_CV, k) = cv;
+        SC(S_CVC, k) = cv;
       }
-      __syncthreads();
-      // ---- reactions at T
-      {
-        const double lprt = SCAL(S_LPRT), invT = SCAL(S_INVT), Csum = SCAL(S_CSUM);
-        for (int r = g; r < m.nrxn; r += NG)
-          reaction_item<TS>(m, m.rxn[r], sl, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
-      }
-      __syncthreads();
-      // ---- net production rates, energy sum
-      double pe = 0.0;
+    }
+    __syncthreads();
+    FORV Csum[k] = SC(S_CSUM, k);
+    // ---- reactions at T
+    for (int r = g; r < m.nrxn; r += NG)
+      reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
+    __syncthreads();
+    // ---- net production rates, energy partial
+    {
+      double pe[V];
+      FORV pe[k] = 0.0;
       for (int s = g; s < S; s += NG) {
-        double des = 0.0, cre = 0.0;
-        for (int k = m.sd_ptr[s]; k < m.sd_ptr[s + 1]; ++k) des += sROP[m.sd_step[k] * TS + sl];
-        for (int k = m.sc_ptr[s]; k < m.sc_ptr[s + 1]; ++k) cre += sROP[m.sc_step[k] * TS + sl];
-        const double net = cre - des;
-        if (valid) {
-          wdot[(size_t)s * ld + st] = net;
-          if (ydot) ydot[(size_t)s * ld + st] = net * m.mw[s] * v;
+        double des[V], cre[V];
+        FORV des[k] = cre[k] = 0.0;
+        gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
+        gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
+        const double mws = m.mw[s];
+        FORV {
+          const double net = cre[k] - des[k];
+          if (valid[k]) {
+            wdot[(size_t)s * ld + st[k]] = net;
+            if (ydot) ydot[(size_t)s * ld + st[k]] = net * mws * v[k];
+          }
+          pe[k] += sU[s * TS + q + k * GS] * net * v[k];
         }
-        pe += sU[s * TS + sl] * net * v;
       }
-      PART(0, g) = pe;
+      FORV pe[k] = warp_group_sum<GS>(pe[k]);
+      if (wlead) FORV PT(0, w, k) = pe[k];
+    }
+    __syncthreads();
+    if (g == 0) {
+      FORV {
+        double es = 0.0;
+        for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
+        const double Td = -es * kRu * SC(S_YS, k) / SC(S_CV, k) + 0.0;
+        SC(S_TDOT, k) = Td;
+        SC(S_TDOTC, k) = Td;
+        if (valid[k] && ydot) ydot[(size_t)S * ld + st[k]] = Td;
+      }
+    }
+    __syncthreads();
+    if (jac == nullptr) continue;
+    // ---- clamped state (reactor_nvector_serial.cpp:629-640), only if needed
+    if (need) {
+      {
+        double pc[V], pcv[V];
+        FORV pc[k] = pcv[k] = 0.0;
+        for (int s = g; s < S; s += NG) {
+          const double *th = m.thermo + 16 * s;
+          const double iw = m.inv_mw[s], riw = m.ru_inv_mw[s];
+          FORV {
+            const double yc = clampy(yload(s, k), kp.mmf);
+            const double c = (1.0 / v[k]) * iw * yc;
+            sX[s * TS + q + k * GS] = c;
+            pc[k] += c;
+            pcv[k] += ((nasa_cp(th, Tr[k]) - 1.0) * riw) * yc;
+          }
+        }
+        FORV {
+          pc[k] = warp_group_sum<GS>(pc[k]);
+          pcv[k] = warp_group_sum<GS>(pcv[k]);
+        }
+        if (wlead) FORV {
+          PT(0, w, k) = pc[k];
+          PT(1, w, k) = pcv[k];
+        }
+      }
       __syncthreads();
       if (g == 0) {
-        double es = 0.0;
-        for (int q = 0; q < NG; ++q) es += PART(0, q);
-        const double Td = -es * kRu * SCAL(S_YS) / SCAL(S_CV) + 0.0;
-        SCAL(S_TDOT) = Td;
-        SCAL(S_TDOTC) = Td;
-        SCAL(S_CVC) = SCAL(S_CV);
-        if (valid && ydot) ydot[(size_t)S * ld + st] = Td;
+        FORV {
+          double cs = 0.0, cv = 0.0;
+          for (int ww = 0; ww < NW; ++ww) {
+            cs += PT(0, ww, k);
+            cv += PT(1, ww, k);
+          }
+          SC(S_CSUM, k) = cs;
+          SC(S_CVC, k) = cv;
+        }
       }
       __syncthreads();
-      if (jac == nullptr) continue;
-      // ---- clamped state (reactor_nvector_serial.cpp:629-640), only if needed
-      if (need) {
-        double pcv2 = 0.0;
-        for (int s = g; s < S; s += NG) {
-          const double y = valid ? Y[(size_t)s * ld + st] : dummy_y;
-          const double yc = clampy(y, kp.mmf);
-          sX[s * TS + sl] = dens * m.inv_mw[s] * yc;
-          const double cvs = (nasa_cp(m.thermo + 16 * s, Tr) - 1.0) * m.ru_inv_mw[s];
-          pcv2 += cvs * yc;
-        }
-        PART(1, g) = pcv2;
-        double pc2 = 0.0;
-        for (int s = g; s < S; s += NG) pc2 += sX[s * TS + sl];
-        PART(0, g) = pc2;
-        __syncthreads();
-        if (g == 0) {
-          double cs = 0.0, cv = 0.0;
-          for (int q = 0; q < NG; ++q) {
-            cs += PART(0, q);
-            cv += PART(1, q);
-          }
-          SCAL(S_CSUM) = cs;
-          SCAL(S_CVC) = cv;
-        }
-        __syncthreads();
-        {
-          const double lprt = SCAL(S_LPRT), invT = SCAL(S_INVT), Csum = SCAL(S_CSUM);
-          for (int r = g; r < m.nrxn; r += NG)
-            reaction_item<TS>(m, m.rxn[r], sl, sX, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
-        }
-        __syncthreads();
-        double pe2 = 0.0;
-        for (int s = g; s < S; s += NG) {
-          double des = 0.0, cre = 0.0;
-          for (int k = m.sd_ptr[s]; k < m.sd_ptr[s + 1]; ++k) des += sROP[m.sd_step[k] * TS + sl];
-          for (int k = m.sc_ptr[s]; k < m.sc_ptr[s + 1]; ++k) cre += sROP[m.sc_step[k] * TS + sl];
-          pe2 += sU[s * TS + sl] * (cre - des) * v;
-        }
-        PART(0, g) = pe2;
-        __syncthreads();
-        if (g == 0) {
-          double es = 0.0;
-          for (int q = 0; q < NG; ++q) es += PART(0, q);
-          SCAL(S_TDOTC) = -es * kRu * SCAL(S_YS) / SCAL(S_CVC) + 0.0;
-        }
-        __syncthreads();
-      }
-      // ---- analytic Jacobian columns + temperature row
       {
-        const double RuTemp = kRu * SCAL(S_YS);
-        const double TdC = SCAL(S_TDOTC);
-        const double multFact = -1.0 / SCAL(S_CVC);
-        for (int j = g; j < S; j += NG) {
-          const double y = valid ? Y[(size_t)j * ld + st] : dummy_y;
-          const double t2 = m.mw[j] / clampy(y, kp.mmf) * v;
-          const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
-          const double cvj = (nasa_cp(m.thermo + 16 * j, Tr) - 1.0) * m.ru_inv_mw[j];
-          const double wcol = m.inv_mw[j];
-          double trow = 0.0;
-          for (int k = k0; k < k1; ++k) {
-            const int row = m.row_idx[k];
-            double val = 0.0;
-            for (int q = m.nzd_ptr[k]; q < m.nzd_ptr[k + 1]; ++q) val -= sROP[m.nzd_step[q] * TS + sl] * t2;
-            for (int q = m.nzc_ptr[k]; q < m.nzc_ptr[k + 1]; ++q) val += sROP[m.nzc_step[q] * TS + sl] * t2;
-            trow += val * sU[row * TS + sl];
-            if (valid) jac[(size_t)k * ld + st] = val * (m.mw[row] * wcol);
-          }
-          double tr = trow * RuTemp;
-          tr += TdC * cvj * m.mw[j];
-          tr *= wcol * multFact;
-          if (valid) jac[(size_t)k1 * ld + st] = tr;
+        double Cc[V];
+        FORV Cc[k] = SC(S_CSUM, k);
+        for (int r = g; r < m.nrxn; r += NG)
+          reaction_item<TS, V>(m, m.rxn[r], q, sX, sG, sROP, Tr, logT, invT, lprt, Cc, kp.lim);
+      }
+      __syncthreads();
+      {
+        double pe[V];
+        FORV pe[k] = 0.0;
+        for (int s = g; s < S; s += NG) {
+          double des[V], cre[V];
+          FORV des[k] = cre[k] = 0.0;
+          gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
+          gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
+          FORV pe[k] += sU[s * TS + q + k * GS] * (cre[k] - des[k]) * v[k];
+        }
+        FORV pe[k] = warp_group_sum<GS>(pe[k]);
+        if (wlead) FORV PT(0, w, k) = pe[k];
+      }
+      __syncthreads();
+      if (g == 0) {
+        FORV {
+          double es = 0.0;
+          for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
+          SC(S_TDOTC, k) = -es * kRu * SC(S_YS, k) / SC(S_CVC, k) + 0.0;
         }
       }
       __syncthreads();
     }
-    if (jac == nullptr) continue;
+    // ---- analytic Jacobian columns + temperature row
+    {
+      double RuTemp[V], TdC[V], multFact[V];
+      FORV {
+        RuTemp[k] = kRu * SC(S_YS, k);
+        TdC[k] = SC(S_TDOTC, k);
+        multFact[k] = -1.0 / SC(S_CVC, k);
+      }
+      for (int j = g; j < S; j += NG) {
+        const double mwj = m.mw[j], wcol = m.inv_mw[j];
+        const double *th = m.thermo + 16 * j;
+        const double riw = m.ru_inv_mw[j];
+        double t2[V], trow[V];
+        FORV {
+          t2[k] = mwj / clampy(yload(j, k), kp.mmf) * v[k];
+          trow[k] = 0.0;
+        }
+        const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
+        for (int kk = k0; kk < k1; ++kk) {
+          const int row = m.row_idx[kk];
+          double des[V], cre[V];
+          FORV des[k] = cre[k] = 0.0;
+          gather_rop<TS, V>(sROP, m.nzd_step, m.nzd_ptr[kk], m.nzd_ptr[kk + 1], q, des);
+          gather_rop<TS, V>(sROP, m.nzc_step, m.nzc_ptr[kk], m.nzc_ptr[kk + 1], q, cre);
+          const double conv = m.mw[row] * wcol;
+          FORV {
+            // destruction terms first, then creation (SetupJacobianSparse order)
+            const double val = (0.0 - des[k] * t2[k]) + cre[k] * t2[k];
+            trow[k] += val * sU[row * TS + q + k * GS];
+            if (valid[k]) jac[(size_t)kk * ld + st[k]] = val * conv;
+          }
+        }
+        FORV {
+          const double cvj = (nasa_cp(th, Tr[k]) - 1.0) * riw;
+          double tr = trow[k] * RuTemp[k];
+          tr += TdC[k] * cvj * mwj;
+          tr *= wcol * multFact[k];
+          if (valid[k]) jac[(size_t)k1 * ld + st[k]] = tr;
+        }
+      }
+    }
+    __syncthreads();
     // ---- temperature-perturbed RHS for the forward-difference column
     if (g == 0) {
-      const double yS = SCAL(S_YS);
-      const double ySp = yS + yS * kp.sqrt_ur;
-      const double dT = ySp - yS;
-      SCAL(S_YSP) = ySp;
-      SCAL(S_MULT) = 1.0 / dT;
-      double Tp = ySp * kp.Tref;
-      if (Tp > 1.0e4) Tp = 1.0e4;
-      SCAL(S_TR) = Tp;
-      SCAL(S_LOGT) = log(Tp);
-      SCAL(S_INVT) = 1.0 / Tp;
-      SCAL(S_LPRT) = log(kPatm / (kRu * Tp));
+      FORV {
+        const double yS = SC(S_YS, k);
+        const double ySp = yS + yS * kp.sqrt_ur;
+        const double dT = ySp - yS;
+        SC(S_YSP, k) = ySp;
+        SC(S_MULT, k) = 1.0 / dT;
+        double Tp = ySp * kp.Tref;
+        if (Tp > 1.0e4) Tp = 1.0e4;
+        SC(S_TR, k) = Tp;
+        SC(S_LOGT, k) = log(Tp);
+        SC(S_INVT, k) = 1.0 / Tp;
+        SC(S_LPRT, k) = log(kPatm / (kRu * Tp));
+      }
+    }
+    __syncthreads();
+    FORV {
+      Tr[k] = SC(S_TR, k);
+      logT[k] = SC(S_LOGT, k);
+      invT[k] = SC(S_INVT, k);
+      lprt[k] = SC(S_LPRT, k);
+    }
+    {
+      double pcv[V];
+      FORV pcv[k] = 0.0;
+      for (int s = g; s < S; s += NG) {
+        const double *th = m.thermo + 16 * s;
+        const double riw = m.ru_inv_mw[s];
+        FORV {
+          double cp, h, gg;
+          nasa_cp_h_g(th, Tr[k], logT[k], &cp, &h, &gg);
+          sG[s * TS + q + k * GS] = gg;
+          sU[s * TS + q + k * GS] = h - 1.0;
+          pcv[k] += ((cp - 1.0) * riw) * yload(s, k);
+        }
+      }
+      FORV pcv[k] = warp_group_sum<GS>(pcv[k]);
+      if (wlead) FORV PT(1, w, k) = pcv[k];
+    }
+    __syncthreads();
+    if (g == 0) {
+      FORV {
+        double cv = 0.0;
+        for (int ww = 0; ww < NW; ++ww) cv += PT(1, ww, k);
+        SC(S_CVP, k) = cv;
+      }
+    }
+    __syncthreads();
+    for (int r = g; r < m.nrxn; r += NG)
+      reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
+    __syncthreads();
+    {
+      double pe[V];
+      FORV pe[k] = 0.0;
+      for (int s = g; s < S; s += NG) {
+        double des[V], cre[V];
+        FORV des[k] = cre[k] = 0.0;
+        gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
+        gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
+        FORV {
+          const double net = cre[k] - des[k];
+          sX[s * TS + q + k * GS] = net;
+          pe[k] += sU[s * TS + q + k * GS] * net * v[k];
+        }
+      }
+      FORV pe[k] = warp_group_sum<GS>(pe[k]);
+      if (wlead) FORV PT(0, w, k) = pe[k];
+    }
+    __syncthreads();
+    if (g == 0) {
+      FORV {
+        double es = 0.0;
+        for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
+        SC(S_TDOTP, k) = -es * kRu * SC(S_YSP, k) / SC(S_CVP, k) + 0.0;
+      }
     }
     __syncthreads();
     {
-      const double Tp = SCAL(S_TR), logTp = SCAL(S_LOGT), v = SCAL(S_V);
-      double pcv = 0.0, pc = 0.0;
-      for (int s = g; s < S; s += NG) {
-        const double y = valid ? Y[(size_t)s * ld + st] : dummy_y;
-        double cp, h, gg;
-        nasa_cp_h_g(m.thermo + 16 * s, Tp, logTp, &cp, &h, &gg);
-        sG[s * TS + sl] = gg;
-        sU[s * TS + sl] = h - 1.0;
-        pcv += ((cp - 1.0) * m.ru_inv_mw[s]) * y;
-        pc += sC[s * TS + sl];
+      double mult[V], tdp[V], td[V];
+      FORV {
+        mult[k] = SC(S_MULT, k);
+        tdp[k] = SC(S_TDOTP, k);
+        td[k] = SC(S_TDOT, k);
       }
-      PART(0, g) = pc;
-      PART(1, g) = pcv;
-      __syncthreads();
-      if (g == 0) {
-        double cs = 0.0, cv = 0.0;
-        for (int q = 0; q < NG; ++q) {
-          cs += PART(0, q);
-          cv += PART(1, q);
-        }
-        SCAL(S_CSUM) = cs;
-        SCAL(S_CVP) = cv;
-      }
-      __syncthreads();
-      {
-        const double lprt = SCAL(S_LPRT), invT = SCAL(S_INVT), Csum = SCAL(S_CSUM);
-        for (int r = g; r < m.nrxn; r += NG)
-          reaction_item<TS>(m, m.rxn[r], sl, sC, sG, sROP, Tp, logTp, invT, lprt, Csum, kp.lim);
-      }
-      __syncthreads();
-      double pe = 0.0;
-      for (int s = g; s < S; s += NG) {
-        double des = 0.0, cre = 0.0;
-        for (int k = m.sd_ptr[s]; k < m.sd_ptr[s + 1]; ++k) des += sROP[m.sd_step[k] * TS + sl];
-        for (int k = m.sc_ptr[s]; k < m.sc_ptr[s + 1]; ++k) cre += sROP[m.sc_step[k] * TS + sl];
-        const double net = cre - des;
-        sX[s * TS + sl] = net;
-        pe += sU[s * TS + sl] * net * v;
-      }
-      PART(0, g) = pe;
-      __syncthreads();
-      if (g == 0) {
-        double es = 0.0;
-        for (int q = 0; q < NG; ++q) es += PART(0, q);
-        SCAL(S_TDOTP) = -es * kRu * SCAL(S_YSP) / SCAL(S_CVP) + 0.0;
-      }
-      __syncthreads();
-      const double mult = SCAL(S_MULT);
       const int k0 = m.col_ptr[S], k1 = m.col_ptr[S + 1];
-      for (int k = k0 + g; k < k1; k += NG) {
-        const int row = m.row_idx[k];
-        double d;
-        if (row < S) {
-          const double f1 = sX[row * TS + sl] * m.mw[row] * v;
-          const double f0 = (valid ? wdot[(size_t)row * ld + st] : 0.0) * m.mw[row] * v;
-          d = (f1 - f0) * mult;
-        } else {
-          d = (SCAL(S_TDOTP) - SCAL(S_TDOT)) * mult;
+      for (int kk = k0 + g; kk < k1; kk += NG) {
+        const int row = m.row_idx[kk];
+        FORV {
+          double d;
+          if (row < S) {
+            const double mr = m.mw[row];
+            const double f1 = sX[row * TS + q + k * GS] * mr * v[k];
+            const double f0 = (valid[k] ? wdot[(size_t)row * ld + st[k]] : 0.0) * mr * v[k];
+            d = (f1 - f0) * mult[k];
+          } else {
+            d = (tdp[k] - td[k]) * mult[k];
+          }
+          if (valid[k]) jac[(size_t)kk * ld + st[k]] = d;
         }
-        if (valid) jac[(size_t)k * ld + st] = d;
       }
-      __syncthreads();
     }
+    __syncthreads();
   }
-#undef SCAL
-#undef PART
+#undef SC
+#undef PT
+#undef FORV
 }
 
-template <int TS>
-cudaError_t launch_ts(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
-                      const LaunchCfg &cfg, cudaStream_t stream) {
+template <int TS, int V, int MAXT>
+cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
+                       const LaunchCfg &cfg, cudaStream_t stream) {
   const int threads = cfg.warps * 32;
-  const int NG = threads / TS;
-  const Layout L = make_layout(m.nsp, m.nstep, NG);
+  const Layout L = make_layout(m.nsp, m.nstep, cfg.warps);
   const size_t ws_bytes = (size_t)L.rows * TS * sizeof(double);
   const int ntiles = (a.n + TS - 1) / TS;
   if (ntiles == 0) return cudaSuccess;
   if (!cfg.global_ws) {
-    cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS>,
+    cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes);
     if (e != cudaSuccess) return e;
-    rates_jac_kernel<TS><<<ntiles, threads, ws_bytes, stream>>>(
+    rates_jac_kernel<TS, V, MAXT><<<ntiles, threads, ws_bytes, stream>>>(
         m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac, a.ydot, kp, nullptr, 0);
   } else {
     int grid = cfg.grid > 0 ? cfg.grid : ntiles;
     if (grid > ntiles) grid = ntiles;
     if ((size_t)grid * ws_bytes > a.scratch_bytes) return cudaErrorInvalidValue;
-    rates_jac_kernel<TS><<<grid, threads, 0, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac,
-                                                      a.ydot, kp, a.scratch,
-                                                      (int)(ws_bytes / sizeof(double)));
+    rates_jac_kernel<TS, V, MAXT><<<grid, threads, 0, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
+                                                         a.jac, a.ydot, kp, a.scratch,
+                                                         (int)(ws_bytes / sizeof(double)));
   }
   return cudaGetLastError();
+}
+
+// Up to 8 warps per CTA the kernel may use 255 registers per thread; with
+// more warps it is compiled for at most 128.
+template <int TS, int V>
+cudaError_t launch_tv(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
+                      const LaunchCfg &cfg, cudaStream_t stream) {
+  if (cfg.warps <= 8) return launch_tvm<TS, V, 256>(m, a, kp, cfg, stream);
+  return launch_tvm<TS, V, 512>(m, a, kp, cfg, stream);
 }
 
 }  // namespace
 
 size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg) {
-  const int NG = cfg.warps * 32 / cfg.ts;
-  const Layout L = make_layout(m.nsp, m.nstep, NG);
+  const Layout L = make_layout(m.nsp, m.nstep, cfg.warps);
   return (size_t)L.rows * cfg.ts * sizeof(double);
+}
+
+bool rates_jac_mapping_ok(const LaunchCfg &c) {
+  if (c.warps < 1 || c.warps > 16) return false;
+  switch (c.ts * 8 + c.v) {
+    case 8 * 8 + 1: case 8 * 8 + 2: case 8 * 8 + 4:
+    case 16 * 8 + 1: case 16 * 8 + 2: case 16 * 8 + 4:
+    case 32 * 8 + 1: case 32 * 8 + 2: case 32 * 8 + 4:
+      return true;
+    default:
+      return false;
+  }
 }
 
 cudaError_t launch_rates_jac(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
                              const LaunchCfg &cfg, cudaStream_t stream) {
-  switch (cfg.ts) {
-    case 8: return launch_ts<8>(m, a, kp, cfg, stream);
-    case 16: return launch_ts<16>(m, a, kp, cfg, stream);
-    case 32: return launch_ts<32>(m, a, kp, cfg, stream);
+  switch (cfg.ts * 8 + cfg.v) {
+    case 8 * 8 + 1: return launch_tv<8, 1>(m, a, kp, cfg, stream);
+    case 8 * 8 + 2: return launch_tv<8, 2>(m, a, kp, cfg, stream);
+    case 8 * 8 + 4: return launch_tv<8, 4>(m, a, kp, cfg, stream);
+    case 16 * 8 + 1: return launch_tv<16, 1>(m, a, kp, cfg, stream);
+    case 16 * 8 + 2: return launch_tv<16, 2>(m, a, kp, cfg, stream);
+    case 16 * 8 + 4: return launch_tv<16, 4>(m, a, kp, cfg, stream);
+    case 32 * 8 + 1: return launch_tv<32, 1>(m, a, kp, cfg, stream);
+    case 32 * 8 + 2: return launch_tv<32, 2>(m, a, kp, cfg, stream);
+    case 32 * 8 + 4: return launch_tv<32, 4>(m, a, kp, cfg, stream);
     default: return cudaErrorInvalidValue;
   }
 }

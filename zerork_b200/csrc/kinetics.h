@@ -15,11 +15,13 @@ struct KinParams {
   double sqrt_ur;  // sqrt(DBL_EPSILON), the forward-difference scale
 };
 
-// Tile / CTA mapping: ts states per tile (8, 16 or 32), warps per CTA, and
+// Tile / CTA mapping: ts states per tile (8, 16 or 32), v states per thread,
+// warps per CTA, and
 // whether the per-tile workspace lives in global scratch (grid CTAs, each
 // with its own slice) instead of shared memory.
 struct LaunchCfg {
   int ts = 16;
+  int v = 1;  // states per thread (1, 2 or 4); ts / v threads share one work item
   int warps = 8;
   bool global_ws = false;
   int grid = 0;
@@ -37,6 +39,7 @@ struct RatesJacArgs {
 };
 
 size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg);
+bool rates_jac_mapping_ok(const LaunchCfg &cfg);
 cudaError_t launch_rates_jac(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
                              const LaunchCfg &cfg, cudaStream_t stream);
 
