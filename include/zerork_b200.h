@@ -104,6 +104,15 @@ int zrk_rates_jac_dev(zrk_mech_t m, int n, int ld, const double *T, const double
 int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, const double *Y,
                        double *wdot, double *jac);
 
+/* Totals of the last zerork_reactor_solve call on a plugin handle
+ * (struct zerork_handle_impl *, include/zerork_cfd_plugin.h): totals7 =
+ * {steps, rejected steps, Newton iterations, Jacobians, factorizations,
+ * right-hand sides, failed reactors}; kernel_ms = integration kernel time.
+ * No counterpart in the reference beyond its per-solve performance log
+ * (zerork_reactor_manager.cpp:1285-1330). */
+struct zerork_handle_impl;
+int zrk_plugin_last_stats(struct zerork_handle_impl *h, long *totals7, float *kernel_ms);
+
 #ifdef __cplusplus
 }
 #endif

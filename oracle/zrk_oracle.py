@@ -53,6 +53,17 @@ class ZoJacPattern(C.Structure):
                 ("cre_step", C.POINTER(C.c_int)), ("cre_nz", C.POINTER(C.c_int))]
 
 
+class ZoBdfOpts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_dt", C.c_double),
+                ("nlscoef", C.c_double), ("max_steps", C.c_int), ("Tref", C.c_double),
+                ("min_mass_frac", C.c_double), ("step_limiter", C.c_double),
+                ("analytic", C.c_int)]
+
+
+class ZoBdfStats(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("nsteps", "nrej", "nnewt", "njac", "nlu", "nrhs", "status")]
+
+
 # array name -> (dtype, size expression over the struct's counts)
 TABLE_ARRAYS = {
     "mw": ("f8", lambda t: t.nsp), "thermo": ("f8", lambda t: 16 * t.nsp),
@@ -95,6 +106,12 @@ def _bind_common(lib):
                                               C.c_int, _dp, _dp, _dp, C.c_double, C.c_double,
                                               C.c_double, _dp, _dp, _dp, _dp]
     lib.zo_batch_rates_jac_scaled.restype = C.c_int
+    if hasattr(lib, "zo_reactor_solve_batch"):
+        lib.zo_bdf_default_opts.argtypes = [C.POINTER(ZoBdfOpts)]
+        lib.zo_reactor_solve_batch.argtypes = [C.POINTER(ZoTables), C.POINTER(ZoJacPattern),
+                                               C.POINTER(ZoBdfOpts), C.c_int, C.c_int, C.c_double,
+                                               _dp, _dp, _dp, C.c_void_p]
+        lib.zo_reactor_solve_batch.restype = C.c_int
     return lib
 
 
@@ -249,6 +266,24 @@ class OracleTables:
         if nf:
             raise RuntimeError(f"oracle batch failed on {nf} states")
         return wdot, jac, ws, js
+
+
+    def solve(self, T, P, Y, dt, nthreads=1, **opts):
+        """Oracle BDF integration of constant-volume reactors (reactor-major Y).
+        Returns (T, P, Y, stats-dict-of-arrays); opts override the plugin defaults."""
+        o = ZoBdfOpts()
+        self.lib.zo_bdf_default_opts(C.byref(o))
+        for k, v in opts.items():
+            setattr(o, k, v)
+        T = np.array(T, dtype=np.float64)
+        P = np.array(P, dtype=np.float64)
+        Y = np.array(Y, dtype=np.float64, order="C")
+        n = T.shape[0]
+        st = (ZoBdfStats * n)()
+        nf = self.lib.zo_reactor_solve_batch(self.ptr, self.pat, C.byref(o), nthreads, n, float(dt),
+                                             T, P, Y, C.cast(st, C.c_void_p))
+        stats = {f: np.array([getattr(st[i], f) for i in range(n)]) for f, _ in ZoBdfStats._fields_}
+        return T, P, Y, stats
 
 
 class RefMechanism:

@@ -1,0 +1,58 @@
+/*
+ * zrk_oracle_bdf.h -- CPU ORACLE integrator (test infrastructure only).
+ *
+ * The reference integrates each reactor with SUNDIALS CVODE (BDF, Newton,
+ * applications/cfd_plugin/solver_cvode.cpp:51-299).  SUNDIALS 5.8.0 is not
+ * vendored in the reference (cmake/sundials5.CMakeLists.txt:8) and cannot be
+ * fetched here, so this oracle restates a published variable-order BDF
+ * instead: the quasi-constant step-size BDF of Shampine & Reichelt, "The
+ * MATLAB ODE Suite", SIAM J. Sci. Comput. 18 (1997) (orders 1-5, modified
+ * Newton iteration, order/step selection after order+1 equal steps), with
+ * CVODE's option semantics from the plugin: rel_tol, abs_tol, max_steps,
+ * max_dt, nonlinear_convergence_coeff (solver_cvode.cpp:66-88).  Newton
+ * matrices are I - c J with J the reactor Jacobian of zrk_oracle.c
+ * (SetupJacobianSparse semantics), factored densely with partial pivoting.
+ * End states are therefore compared to the GPU integrator at the integration
+ * tolerance, not step by step (CVODE's step sequence is unpinned).
+ */
+#ifndef ZRK_ORACLE_BDF_H
+#define ZRK_ORACLE_BDF_H
+
+#include "zrk_oracle.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct zo_bdf_opts {
+  double rtol, atol, max_dt, nlscoef;
+  int max_steps;
+  double Tref, min_mass_frac, step_limiter;
+  int analytic; /* 1: SetupJacobianSparse values; 0: dense divided differences
+                   (the plugin's analytic = 0, reactor_nvector_serial.cpp:360) */
+} zo_bdf_opts;
+
+typedef struct zo_bdf_stats {
+  int nsteps, nrej, nnewt, njac, nlu, nrhs, status; /* status 0 ok, <0 failure */
+} zo_bdf_stats;
+
+void zo_bdf_default_opts(zo_bdf_opts *o);
+
+/* Integrate one constant-volume reactor from (T, P, Y) for dt seconds:
+ * InitializeState / Integrate / GetState of the cfd_plugin
+ * (reactor_constant_volume_cpu.cpp:15-61, zerork_reactor_manager.cpp:1090-1146).
+ * On return T, P, Y hold the end state. */
+int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
+                     const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
+                     zo_bdf_stats *st);
+
+/* Batch over reactors (reactor-major Y [n][nsp]) with nthreads OpenMP
+ * threads, one reactor object per thread; stats may be NULL. */
+int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
+                           int nthreads, int n, double dt, double *T, double *P, double *Y,
+                           zo_bdf_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,110 @@
+"""GPU batched integrator through the cfd_plugin C ABI, against the CPU oracle.
+
+The oracle (oracle/zrk_bdf.c) integrates the same reactors with the same BDF
+method but dense pivoted LU on the CPU; the GPU uses the warp-level sparse LU
+with static pivots, so step sequences differ and end states are compared at
+the integration tolerance: both are also compared with a tight-tolerance
+oracle run (rtol 1e-12), and the GPU error must be within
+  |T_gpu - T_tight| <= 20 * |T_oracle - T_tight| + 1e-6 * T
+  max_k |Y_gpu - Y_tight| <= 20 * max_k |Y_oracle - Y_tight| + 1e-9
+per reactor (the oracle's own rtol-1e-8 error sets the scale).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import have_gpu, oracle_tables, synth
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def gpu():
+    if not have_gpu():
+        pytest.skip("no CUDA device")
+    return True
+
+
+def _solve(mf, tf, T, P, Y, dt, **opts):
+    from zerork_b200.plugin import Plugin
+    p = Plugin(mf, tf, **opts)
+    Tg, Pg, Yg = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
+    return rc, Tg, Pg, Yg, p
+
+
+def _check_against_tight(ot, T, P, Y, dt, Tg, Yg):
+    nt = os.cpu_count() or 1
+    To, Po, Yo, so = ot.solve(T, P, Y, dt, nthreads=nt)
+    Tt, Pt, Yt, st = ot.solve(T, P, Y, dt, nthreads=nt, rtol=1e-12, atol=1e-24, max_steps=400000)
+    ok = (so["status"] == 0) & (st["status"] == 0)
+    assert ok.sum() >= max(1, len(T) // 2)
+    eo_T = np.abs(To - Tt)[ok]
+    eg_T = np.abs(Tg - Tt)[ok]
+    eo_Y = np.max(np.abs(Yo - Yt), axis=1)[ok]
+    eg_Y = np.max(np.abs(Yg - Yt), axis=1)[ok]
+    assert np.all(eg_T <= 20 * eo_T + 1e-6 * Tt[ok]), (eg_T, eo_T)
+    assert np.all(eg_Y <= 20 * eo_Y + 1e-9), (eg_Y, eo_Y)
+    return eg_T, eg_Y
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_c1_end_states(gpu, fp32, mech_dir):
+    from zerork_b200 import mechgen
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 16, "c1", seed=11)
+    rc, Tg, Pg, Yg, p = _solve(mf, tf, T, P, Y, 1e-3, lu_fp32=fp32)
+    assert rc == 0
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    _check_against_tight(ot, T, P, Y, 1e-3, Tg, Yg)
+    st = p.last_stats()
+    assert st["nfailed"] == 0 and st["nsteps"] > 0
+    # mass fractions stay normalised; pressure from the ideal gas at fixed density
+    assert np.allclose(Yg.sum(axis=1), 1.0, atol=1e-8)
+
+
+def test_c3_subset_end_states(gpu, mech_dir):
+    from zerork_b200 import mechgen
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c3_160", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 6, "c3", seed=5)
+    rc, Tg, Pg, Yg, p = _solve(mf, tf, T, P, Y, 2e-4, lu_fp32=1)
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    _check_against_tight(ot, T, P, Y, 2e-4, Tg, Yg)
+
+
+def test_failure_leaves_state_and_reports(gpu, mech_dir):
+    """max_steps too small: FAILED_SOLVE, state unchanged, negative cost
+    (zerork_reactor_manager.cpp:1123-1137)."""
+    from zerork_b200 import mechgen
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 8, "c1", seed=3)
+    from zerork_b200.plugin import Plugin
+    p = Plugin(mf, tf, max_steps=3, cvode_num_retries=1)
+    cost = p.set_aux_field("COST", np.zeros(8))
+    Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+    rc = p.solve(1e-3, Tg, Pg, Yg, raise_on_fail=False)
+    assert rc == 7  # FAILED_SOLVE
+    assert np.array_equal(Tg, T) and np.array_equal(Yg, Y) and np.array_equal(Pg, P)
+    assert np.all(cost < 0)
+
+
+def test_cost_and_temperature_delta_fields(gpu, mech_dir):
+    from zerork_b200 import mechgen
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 8, "c1", seed=4)
+    from zerork_b200.plugin import Plugin
+    p = Plugin(mf, tf)
+    cost = p.set_aux_field("COST", np.ones(8))
+    tdel = p.set_aux_field("TEMPERATURE_DELTA", np.zeros(8))
+    Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+    assert p.solve(1e-3, Tg, Pg, Yg) == 0
+    assert np.all(cost > 0)
+    d = Tg - T
+    assert np.allclose(tdel, np.where(d < 2.0, 0.0, d))
+    # second call reuses the cost ordering and gives the same answer
+    T2, P2, Y2 = T.copy(), P.copy(), Y.copy()
+    assert p.solve(1e-3, T2, P2, Y2) == 0
+    assert np.array_equal(T2, Tg) and np.array_equal(Y2, Yg)

@@ -1,0 +1,570 @@
+// integrator.cu -- warp-per-reactor BDF integration of constant-volume
+// reactors (see integrator.h).
+//
+// Per warp: the reactor's right-hand side (reactor_constant_volume_cpu.cpp:
+// 64-128) with lanes over species and reactions; its Jacobian
+// (reactor_nvector_serial.cpp:610-771) with lanes over the nonzeros of each
+// column; the Newton matrix P = I - cJ assembled into the fill pattern and
+// factored left-looking with lanes over the entries of each update column;
+// column-oriented triangular solves; WRMS norms by shuffle reductions.  All
+// lanes hold identical copies of the step-control scalars (reduced values are
+// broadcast from lane 0), so control flow is warp-uniform.
+#include <cuda_runtime.h>
+
+#include "integrator.h"
+#include "kinetics_dev.cuh"
+
+namespace zrk {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kNewtonMaxIter = 3;
+constexpr double kMinFactor = 0.2;
+constexpr double kMaxFactor = 10.0;
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return __shfl_sync(kFull, v, 0);
+}
+
+struct Warp {
+  double *C, *G, *U, *ROP;  // species rows and rates of progress
+  void *X;                  // LU work / solve vector (n elements of the LU type)
+};
+
+struct BdfConst {
+  double gam[kMaxOrder + 2], alp[kMaxOrder + 2], econ[kMaxOrder + 2];
+};
+
+__device__ void bdf_consts(BdfConst &b) {
+  const double kap[kMaxOrder + 1] = {0.0, -0.1850, -1.0 / 9.0, -0.0823, -0.0415, 0.0};
+  for (int k = 0; k <= kMaxOrder + 1; ++k) {
+    double g = 0.0;
+    for (int i = 1; i <= k; ++i) g += 1.0 / i;
+    b.gam[k] = g;
+    const double kk = (k <= kMaxOrder) ? kap[k] : 0.0;
+    b.alp[k] = (1.0 - kk) * g;
+    b.econ[k] = kk * g + 1.0 / (k + 1);
+  }
+}
+
+// ydot at y (global or shared vector of nsp+1 entries); returns 1 if T <= 0.
+__device__ int rhs_warp(const DevMech &m, const IntegOpts &o, const Warp &w, double v,
+                        const double *y, double *ydot, int lane, bool clamp, double *cv_out) {
+  const int S = m.nsp;
+  const double yS = y[S];
+  double T = yS * o.Tref;
+  if (!(T > 0.0)) return 1;
+  if (T > 1.0e4) T = 1.0e4;
+  const double logT = log(T), invT = 1.0 / T, lprt = log(kPatmD / (kRuD * T));
+  const double dens = 1.0 / v;
+  double pc = 0.0, pcv = 0.0;
+  for (int s = lane; s < S; s += 32) {
+    double ys = y[s];
+    if (clamp) ys = clamp_mass_fraction(ys, o.mmf);
+    const double c = dens * m.inv_mw[s] * ys;
+    w.C[s] = c;
+    double cp, h, g;
+    nasa_cp_h_g(m.thermo + 16 * s, T, logT, &cp, &h, &g);
+    w.G[s] = g;
+    w.U[s] = h - 1.0;
+    pc += c;
+    pcv += ((cp - 1.0) * m.ru_inv_mw[s]) * ys;
+  }
+  const double Csum = wsum(pc), cv = wsum(pcv);
+  __syncwarp();
+  for (int r = lane; r < m.nrxn; r += 32)
+    reaction_item<1, 1>(m, m.rxn[r], 0, w.C, w.G, w.ROP, &T, &logT, &invT, &lprt, &Csum, o.lim);
+  __syncwarp();
+  double pe = 0.0;
+  for (int s = lane; s < S; s += 32) {
+    double des = 0.0, cre = 0.0;
+    for (int k = m.sd_ptr[s]; k < m.sd_ptr[s + 1]; ++k) des += w.ROP[m.sd_step[k]];
+    for (int k = m.sc_ptr[s]; k < m.sc_ptr[s + 1]; ++k) cre += w.ROP[m.sc_step[k]];
+    const double net = cre - des;
+    ydot[s] = net * m.mw[s] * v;
+    pe += w.U[s] * net * v;
+  }
+  const double es = wsum(pe);
+  if (lane == 0) ydot[S] = -es * kRuD * yS / cv + 0.0;
+  if (cv_out) *cv_out = cv;
+  __syncwarp();
+  return 0;
+}
+
+// Jacobian values J[nnz] at y with fy = ydot(y); tmp: nsp+1 global doubles,
+// yp: nsp+1 shared/global doubles of scratch.
+__device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, double v,
+                        const double *y, const double *fy, double *J, double *tmp, double *yp,
+                        int lane) {
+  const int S = m.nsp;
+  int need = 0;
+  for (int s = lane; s < S; s += 32) need |= (fabs(y[s]) < o.mmf);
+  need = __any_sync(kFull, need);
+  double cvc;
+  if (rhs_warp(m, o, w, v, y, tmp, lane, need != 0, &cvc)) return 1;
+  const double TdC = tmp[S];
+  const double yS = y[S];
+  const double RuTemp = kRuD * yS;
+  const double multFact = -1.0 / cvc;
+  double T = yS * o.Tref;
+  if (T > 1.0e4) T = 1.0e4;
+  for (int j = 0; j < S; ++j) {
+    const double t2 = m.mw[j] / clamp_mass_fraction(y[j], o.mmf) * v;
+    const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
+    const double wcol = m.inv_mw[j];
+    double trow = 0.0;
+    for (int kk = k0 + lane; kk < k1; kk += 32) {
+      const int row = m.row_idx[kk];
+      double des = 0.0, cre = 0.0;
+      for (int q = m.nzd_ptr[kk]; q < m.nzd_ptr[kk + 1]; ++q) des += w.ROP[m.nzd_step[q]];
+      for (int q = m.nzc_ptr[kk]; q < m.nzc_ptr[kk + 1]; ++q) cre += w.ROP[m.nzc_step[q]];
+      const double val = (0.0 - des * t2) + cre * t2;
+      trow += val * w.U[row];
+      J[kk] = val * (m.mw[row] * wcol);
+    }
+    trow = wsum(trow);
+    if (lane == 0) {
+      const double cvj = (nasa_cp(m.thermo + 16 * j, T) - 1.0) * m.ru_inv_mw[j];
+      double tr = trow * RuTemp;
+      tr += TdC * cvj * m.mw[j];
+      tr *= wcol * multFact;
+      J[k1] = tr;
+    }
+  }
+  __syncwarp();
+  // forward-difference temperature column
+  const double ySp = yS + yS * o.sqrt_ur;
+  const double mult = 1.0 / (ySp - yS);
+  for (int s = lane; s < S; s += 32) yp[s] = y[s];
+  if (lane == 0) yp[S] = ySp;
+  __syncwarp();
+  if (rhs_warp(m, o, w, v, yp, tmp, lane, false, nullptr)) return 1;
+  for (int kk = m.col_ptr[S] + lane; kk < m.col_ptr[S + 1]; kk += 32) {
+    const int row = m.row_idx[kk];
+    J[kk] = (tmp[row] - fy[row]) * mult;
+  }
+  __syncwarp();
+  return 0;
+}
+
+// P = I - cJ into the LU storage, then left-looking factorization in place.
+template <class LT>
+__device__ int lu_factor_warp(const LUDev &lu, const double *J, int jnnz, double c, LT *LU, LT *x,
+                              int lane) {
+  for (int p = lane; p < lu.nnz; p += 32) LU[p] = (LT)0;
+  __syncwarp();
+  for (int k = lane; k < jnnz; k += 32) LU[lu.jac_to_lu[k]] = (LT)(-c * J[k]);
+  __syncwarp();
+  for (int i = lane; i < lu.n; i += 32) LU[lu.diag_of_orig[i]] += (LT)1;
+  __syncwarp();
+  int bad = 0;
+  for (int j = 0; j < lu.n; ++j) {
+    const int p0 = lu.col_ptr[j], p1 = lu.col_ptr[j + 1], dj = lu.diag[j];
+    for (int p = p0 + lane; p < p1; p += 32) x[lu.row_idx[p]] = LU[p];
+    __syncwarp();
+    for (int p = p0; p < dj; ++p) {
+      const int k = lu.row_idx[p];
+      const LT xk = x[k];
+      if (xk != (LT)0)
+        for (int q = lu.diag[k] + 1 + lane; q < lu.col_ptr[k + 1]; q += 32)
+          x[lu.row_idx[q]] -= LU[q] * xk;
+      __syncwarp();
+    }
+    const LT piv = x[j];
+    if (!(piv != (LT)0) || !isfinite((double)piv)) bad = 1;
+    const LT inv = (LT)1 / piv;
+    for (int p = p0 + lane; p < p1; p += 32) {
+      const int r = lu.row_idx[p];
+      const LT val = x[r];
+      LU[p] = (r > j) ? val * inv : val;
+    }
+    __syncwarp();
+  }
+  return bad;
+}
+
+// x <- P^{-1} x in permuted ordering (x in shared memory).
+template <class LT>
+__device__ void lu_solve_warp(const LUDev &lu, const LT *LU, LT *x, int lane) {
+  for (int k = 0; k < lu.n; ++k) {
+    const LT xk = x[k];
+    if (xk != (LT)0)
+      for (int q = lu.diag[k] + 1 + lane; q < lu.col_ptr[k + 1]; q += 32)
+        x[lu.row_idx[q]] -= LU[q] * xk;
+    __syncwarp();
+  }
+  for (int k = lu.n - 1; k >= 0; --k) {
+    const LT xk = x[k] / LU[lu.diag[k]];
+    __syncwarp();
+    if (lane == 0) x[k] = xk;
+    if (xk != (LT)0)
+      for (int q = lu.col_ptr[k] + lane; q < lu.diag[k]; q += 32) x[lu.row_idx[q]] -= LU[q] * xk;
+    __syncwarp();
+  }
+}
+
+// D[0..order] <- (R(factor) U)^T D[0..order], lanes over the n columns.
+__device__ void change_D(double *D, int n, int order, double fac, int lane) {
+  double R[kMaxOrder + 1][kMaxOrder + 1], U[kMaxOrder + 1][kMaxOrder + 1];
+  for (int pass = 0; pass < 2; ++pass) {
+    const double f = pass == 0 ? fac : 1.0;
+    double (*A)[kMaxOrder + 1] = pass == 0 ? R : U;
+    for (int j = 0; j <= order; ++j) {
+      A[0][j] = 1.0;
+      for (int i = 1; i <= order; ++i) A[i][j] = A[i - 1][j] * (j == 0 ? 0.0 : (i - 1 - f * j) / i);
+    }
+  }
+  double RU[kMaxOrder + 1][kMaxOrder + 1];
+  for (int i = 0; i <= order; ++i)
+    for (int j = 0; j <= order; ++j) {
+      double s = 0.0;
+      for (int k = 0; k <= order; ++k) s += R[i][k] * U[k][j];
+      RU[i][j] = s;
+    }
+  for (int mcol = lane; mcol < n; mcol += 32) {
+    double old[kMaxOrder + 1];
+    for (int k = 0; k <= order; ++k) old[k] = D[k * n + mcol];
+    for (int i = 0; i <= order; ++i) {
+      double s = 0.0;
+      for (int k = 0; k <= order; ++k) s += RU[k][i] * old[k];
+      D[i * n + mcol] = s;
+    }
+  }
+  __syncwarp();
+}
+
+struct Vecs {
+  double *D, *y, *f, *f0, *ypred, *psi, *d, *scale, *tmp, *J;
+};
+
+__device__ __forceinline__ double wrms_scaled(const double *x, const double *s, int n, int lane) {
+  double a = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double t = x[i] / s[i];
+    a += t * t;
+  }
+  return sqrt(wsum(a) / n);
+}
+
+// One integration attempt from t = 0 to t_end; y holds the start state and,
+// on return, the last accepted state.  Returns 0 or a negative failure code.
+template <class LT>
+__device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o, const BdfConst &bc,
+                           const Warp &w, const Vecs &V, LT *LU, double v, double t_end,
+                           double rtol, double atol, ReactorStats &st, int lane) {
+  const int n = m.nsp + 1;
+  const int jnnz = m.nnz;
+  LT *x = (LT *)w.X;
+  double t = 0.0;
+  // f0 = f(y0); initial step (Hairer-Norsett-Wanner)
+  st.nrhs++;
+  if (rhs_warp(m, o, w, v, V.y, V.f0, lane, false, nullptr)) return -1;
+  for (int i = lane; i < n; i += 32) V.scale[i] = atol + fabs(V.y[i]) * rtol;
+  __syncwarp();
+  const double d0 = wrms_scaled(V.y, V.scale, n, lane), d1 = wrms_scaled(V.f0, V.scale, n, lane);
+  double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
+  if (h0 > t_end) h0 = t_end;
+  for (int i = lane; i < n; i += 32) V.tmp[i] = V.y[i] + h0 * V.f0[i];
+  __syncwarp();
+  double d2 = 0.0;
+  st.nrhs++;
+  if (rhs_warp(m, o, w, v, V.tmp, V.f, lane, false, nullptr) == 0) {
+    for (int i = lane; i < n; i += 32) V.d[i] = V.f[i] - V.f0[i];
+    __syncwarp();
+    d2 = wrms_scaled(V.d, V.scale, n, lane) / h0;
+  }
+  double h1 = (d1 <= 1e-15 && d2 <= 1e-15) ? fmax(1e-6, h0 * 1e-3) : sqrt(0.01 / fmax(d1, d2));
+  double h = fmin(100.0 * h0, h1);
+  h = fmin(h, o.max_dt);
+  h = fmin(h, t_end);
+  int q = 1, neq = 0;
+  for (int i = lane; i < (kMaxOrder + 3) * n; i += 32) V.D[i] = 0.0;
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) {
+    V.D[i] = V.y[i];
+    V.D[n + i] = V.f0[i] * h;
+  }
+  __syncwarp();
+  st.njac++;
+  if (jac_warp(m, o, w, v, V.y, V.f0, V.J, V.tmp, V.d, lane)) return -2;
+  int jac_current = 1;
+  double c_lu = h / bc.alp[q];
+  st.nlu++;
+  if (lu_factor_warp<LT>(lu, V.J, jnnz, c_lu, LU, x, lane)) return -3;
+  double crate = 1.0;
+  int nsteps = 0;
+  while (t < t_end) {
+    if (nsteps >= o.max_steps) return -4;
+    bool accepted = false;
+    double safety = 0.9, err_norm = 0.0;
+    while (!accepted) {
+      if (h > o.max_dt) {
+        change_D(V.D, n, q, o.max_dt / h, lane);
+        h = o.max_dt;
+      }
+      if (t + h > t_end) {
+        change_D(V.D, n, q, (t_end - t) / h, lane);
+        h = t_end - t;
+      }
+      if (!(t + h > t)) return -5;  // no progress (or h not finite)
+      const double t_new = t + h;
+      for (int i = lane; i < n; i += 32) {
+        double s = 0.0, ps = 0.0;
+        for (int k = 0; k <= q; ++k) s += V.D[k * n + i];
+        for (int k = 1; k <= q; ++k) ps += bc.gam[k] * V.D[k * n + i];
+        V.ypred[i] = s;
+        V.psi[i] = ps / bc.alp[q];
+        V.scale[i] = atol + rtol * fabs(s);
+        V.y[i] = s;
+        V.d[i] = 0.0;
+      }
+      __syncwarp();
+      const double c = h / bc.alp[q];
+      if (fabs(c / c_lu - 1.0) > 0.3) {
+        st.nlu++;
+        c_lu = c;
+        crate = 1.0;
+        if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) return -3;
+      }
+      const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
+      bool conv = false;
+      int it;
+      double dnorm_old = -1.0;
+      for (it = 0; it < kNewtonMaxIter; ++it) {
+        st.nrhs++;
+        if (rhs_warp(m, o, w, v, V.y, V.f, lane, false, nullptr)) break;
+        bool finite = true;
+        for (int i = lane; i < n; i += 32) finite &= isfinite(V.f[i]);
+        if (!__all_sync(kFull, finite)) break;
+        if (it == 0)
+          for (int i = lane; i < n; i += 32) V.f0[i] = V.f[i];
+        st.nnewt++;
+        for (int i = lane; i < n; i += 32)
+          x[lu.iperm[i]] = (LT)(c * V.f[i] - V.psi[i] - V.d[i]);
+        __syncwarp();
+        lu_solve_warp<LT>(lu, LU, x, lane);
+        double a = 0.0;
+        for (int i = lane; i < n; i += 32) {
+          const double dy = (double)x[lu.iperm[i]] * gscale;
+          V.y[i] += dy;
+          V.d[i] += dy;
+          const double tt = dy / V.scale[i];
+          a += tt * tt;
+        }
+        const double dn = sqrt(wsum(a) / n);
+        __syncwarp();
+        if (dnorm_old > 0.0) crate = fmax(0.3 * crate, dn / dnorm_old);
+        if (bc.econ[q] * dn * fmin(1.0, crate) <= o.nlscoef) {
+          conv = true;
+          ++it;
+          break;
+        }
+        if (dnorm_old > 0.0 && dn > 2.0 * dnorm_old) break;
+        dnorm_old = dn;
+      }
+      if (!conv) {
+        if (!jac_current) {
+          st.nrhs++;
+          if (rhs_warp(m, o, w, v, V.ypred, V.f0, lane, false, nullptr)) return -6;
+          st.njac++;
+          if (jac_warp(m, o, w, v, V.ypred, V.f0, V.J, V.tmp, V.f, lane)) return -2;
+          jac_current = 1;
+          st.nlu++;
+          c_lu = c;
+          crate = 1.0;
+          if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) return -3;
+          continue;
+        }
+        change_D(V.D, n, q, 0.5, lane);
+        h *= 0.5;
+        st.nrej++;
+        continue;
+      }
+      safety = 0.9 * (2 * kNewtonMaxIter + 1) / (2.0 * kNewtonMaxIter + it);
+      double a = 0.0;
+      for (int i = lane; i < n; i += 32) {
+        const double e = bc.econ[q] * V.d[i] / V.scale[i];
+        a += e * e;
+      }
+      err_norm = sqrt(wsum(a) / n);
+      if (!isfinite(err_norm)) return -7;
+      if (err_norm > 1.0) {
+        const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
+        change_D(V.D, n, q, fac, lane);
+        h *= fac;
+        st.nrej++;
+        continue;
+      }
+      accepted = true;
+      t = t_new;
+    }
+    ++nsteps;
+    st.nsteps++;
+    ++neq;
+    jac_current = 0;
+    for (int i = lane; i < n; i += 32) {
+      const double di = V.d[i];
+      V.D[(q + 2) * n + i] = di - V.D[(q + 1) * n + i];
+      V.D[(q + 1) * n + i] = di;
+      for (int k = q; k >= 0; --k) V.D[k * n + i] += V.D[(k + 1) * n + i];
+    }
+    __syncwarp();
+    if (neq < q + 1) continue;
+    double em = INFINITY, ep = INFINITY;
+    if (q > 1) {
+      double a = 0.0;
+      for (int i = lane; i < n; i += 32) {
+        const double e = bc.econ[q - 1] * V.D[q * n + i] / V.scale[i];
+        a += e * e;
+      }
+      em = sqrt(wsum(a) / n);
+    }
+    if (q < kMaxOrder) {
+      double a = 0.0;
+      for (int i = lane; i < n; i += 32) {
+        const double e = bc.econ[q + 1] * V.D[(q + 2) * n + i] / V.scale[i];
+        a += e * e;
+      }
+      ep = sqrt(wsum(a) / n);
+    }
+    const double fm = (q > 1) ? pow(em, -1.0 / q) : 0.0;
+    const double f0 = pow(err_norm, -1.0 / (q + 1));
+    const double fp = (q < kMaxOrder) ? pow(ep, -1.0 / (q + 2)) : 0.0;
+    int dq = 0;
+    double best = f0;
+    if (fm > best) { best = fm; dq = -1; }
+    if (fp > best) { best = fp; dq = 1; }
+    q += dq;
+    const double fac = fmin(kMaxFactor, safety * best);
+    change_D(V.D, n, q, fac, lane);
+    h *= fac;
+    neq = 0;
+  }
+  for (int i = lane; i < n; i += 32) V.y[i] = V.D[i];
+  __syncwarp();
+  return 0;
+}
+
+template <class LT>
+__global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, IntegOpts o,
+                                                        IntegArgs a, int rop_in_smem,
+                                                        int per_warp) {
+  extern __shared__ double smem_dyn[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int S = m.nsp, n = S + 1, N = m.nstep;
+  double *base = smem_dyn + wid * per_warp;
+  Warp w;
+  w.C = base;
+  w.G = base + S;
+  w.U = base + 2 * S;
+  double *after = base + 3 * S;
+  if (rop_in_smem) {
+    w.ROP = after;
+    after += N;
+  } else {
+    const int slot = blockIdx.x * (blockDim.x >> 5) + wid;
+    w.ROP = a.rop_scratch + (size_t)slot * N;
+  }
+  w.X = after;
+  BdfConst bc;
+  bdf_consts(bc);
+  for (;;) {
+    int idx = 0;
+    if (lane == 0) idx = atomicAdd(a.queue_head, 1);
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= a.n_reactors) break;
+    const int r = a.order ? a.order[idx] : idx;
+    double *st = a.state + (size_t)r * a.state_stride;
+    Vecs V;
+    V.D = st;
+    V.y = st + (kMaxOrder + 3) * n;
+    V.f = V.y + n;
+    V.f0 = V.f + n;
+    V.ypred = V.f0 + n;
+    V.psi = V.ypred + n;
+    V.d = V.psi + n;
+    V.scale = V.d + n;
+    V.tmp = V.scale + n;
+    V.J = V.tmp + n;
+    LT *LU = (LT *)a.lu + (size_t)r * a.lu_stride;
+    // InitializeState (reactor_constant_volume_cpu.cpp:15-41)
+    const double T0 = a.T[r], P0 = a.P[r];
+    const double *Y0 = a.Y + (size_t)r * S;
+    double pa = 0.0;
+    for (int s = lane; s < S; s += 32) pa += Y0[s] * m.inv_mw[s];
+    const double mwmix = 1.0 / wsum(pa);
+    const double v = 1.0 / (P0 * mwmix / (kRuD * T0));
+    for (int s = lane; s < S; s += 32) V.y[s] = Y0[s];
+    if (lane == 0) V.y[S] = T0 / o.Tref;
+    __syncwarp();
+    ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
+    double rtol = o.rtol, atol = o.atol;
+    int rc = 0;
+    for (int attempt = 0;; ++attempt) {
+      rc = bdf_attempt<LT>(m, lu, o, bc, w, V, LU, v, a.dt, rtol, atol, rs, lane);
+      if (rc == 0 || attempt + 1 >= o.max_retries) break;
+      // solver_cvode.cpp:236-246: adjust tolerances and start over from the
+      // last accepted state for the remaining time
+      rs.retries++;
+      atol *= o.retry_atol_factor;
+      rtol *= o.retry_rtol_factor;
+    }
+    rs.status = rc;
+    // GetState (reactor_constant_volume_cpu.cpp:43-61)
+    if (rc == 0) {
+      double pb = 0.0;
+      for (int s = lane; s < S; s += 32) {
+        const double ys = V.y[s];
+        a.Y[(size_t)r * S + s] = ys;
+        pb += ys * m.inv_mw[s];
+      }
+      const double Tn = V.y[S] * o.Tref;
+      const double mw2 = 1.0 / wsum(pb);
+      if (lane == 0) {
+        a.T[r] = Tn;
+        a.P[r] = kRuD * Tn / (v * mw2);
+      }
+    }
+    if (lane == 0) {
+      a.v[r] = v;
+      if (a.stats) a.stats[r] = rs;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem) {
+  size_t d = 3 * (size_t)m.nsp + (rop_in_smem ? m.nstep : 0) + lu.n + 1;
+  return ((d * sizeof(double) + 15) / 16) * 16;
+}
+
+long integ_state_doubles(const DevMech &m, const LUDev &lu) {
+  const long n = m.nsp + 1;
+  return (kMaxOrder + 3) * n + 8 * n + m.nnz;
+}
+
+cudaError_t launch_integrate(const DevMech &m, const LUDev &lu, const IntegOpts &o,
+                             const IntegArgs &a, int warps_per_cta, int ctas, bool rop_in_smem,
+                             cudaStream_t stream) {
+  const size_t smem = integ_smem_per_warp(m, lu, rop_in_smem) * warps_per_cta;
+  const int pw = (int)(integ_smem_per_warp(m, lu, rop_in_smem) / sizeof(double));
+  cudaError_t e;
+  if (o.lu_fp32) {
+    e = cudaFuncSetAttribute(integrate_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    integrate_kernel<float><<<ctas, warps_per_cta * 32, smem, stream>>>(m, lu, o, a, rop_in_smem, pw);
+  } else {
+    e = cudaFuncSetAttribute(integrate_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    if (e != cudaSuccess) return e;
+    integrate_kernel<double><<<ctas, warps_per_cta * 32, smem, stream>>>(m, lu, o, a, rop_in_smem, pw);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace zrk

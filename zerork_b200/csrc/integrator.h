@@ -1,0 +1,65 @@
+// integrator.h -- batched stiff reactor integration on sm_100a.
+//
+// One warp integrates one constant-volume reactor at a time with a
+// variable-order BDF (orders 1-5, quasi-constant step size, Shampine &
+// Reichelt 1997) and a modified Newton iteration with CVODE's convergence
+// test (Hindmarsh et al., ACM TOMS 2005), the Newton matrix I - cJ built from
+// the reactor Jacobian of reactor_nvector_serial.cpp:610-771 and factored by
+// the warp over the fixed symbolic pattern (sparse_lu.h).  Warps take
+// reactors from a work queue until it is empty: one persistent launch per
+// solve call, each reactor with its own step size, order and Jacobian age.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "devmech.h"
+#include "kinetics.h"
+
+namespace zrk {
+
+constexpr int kMaxOrder = 5;
+
+struct LUDev {
+  int n, nnz;
+  const int *col_ptr, *row_idx, *diag;  // permuted CSC of L+U
+  const int *iperm;                     // original variable -> permuted
+  const int *jac_to_lu;                 // Jacobian nonzero -> LU storage index
+  const int *diag_of_orig;              // original variable -> LU diagonal index
+};
+
+struct IntegOpts {
+  double rtol, atol, max_dt, nlscoef;
+  int max_steps, max_retries;
+  double retry_atol_factor, retry_rtol_factor;
+  double Tref, mmf, lim, sqrt_ur;
+  int lu_fp32;  // factor and apply the Newton matrix in FP32
+};
+
+// Per-reactor statistics written by the kernel.
+struct ReactorStats {
+  int nsteps, nrej, nnewt, njac, nlu, nrhs, status, retries;
+};
+
+struct IntegArgs {
+  int n_reactors;
+  const int *order;         // queue order (reactor indices), may be null
+  int *queue_head;          // device counter, zero before launch
+  double dt;
+  double *T, *P, *Y;        // in/out, Y reactor-major [n_reactors][nsp]
+  double *v;                // inverse densities (filled by the kernel)
+  double *state;            // per-reactor workspace, state_stride doubles each
+  long state_stride;
+  void *lu;                 // per-reactor LU values (double or float), lu_stride elements
+  long lu_stride;
+  ReactorStats *stats;
+  double *rop_scratch;      // optional global ROP rows (one per warp slot)
+};
+
+size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);
+long integ_state_doubles(const DevMech &m, const LUDev &lu);
+cudaError_t launch_integrate(const DevMech &m, const LUDev &lu, const IntegOpts &o,
+                             const IntegArgs &a, int warps_per_cta, int ctas, bool rop_in_smem,
+                             cudaStream_t stream);
+
+}  // namespace zrk

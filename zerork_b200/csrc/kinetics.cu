@@ -25,13 +25,14 @@
 
 #include "devmech.h"
 #include "kinetics.h"
+#include "kinetics_dev.cuh"
 
 namespace zrk {
 
 namespace {
 
-constexpr double kRu = 8.314462618e3;
-constexpr double kPatm = 1.01325e5;
+constexpr double kRu = kRuD;
+constexpr double kPatm = kPatmD;
 
 enum Scal {
   S_T, S_P, S_YS, S_V, S_TR, S_LOGT, S_INVT, S_LPRT, S_CSUM, S_CV, S_TDOT, S_CVC, S_TDOTC,
@@ -54,169 +55,6 @@ __host__ __device__ inline Layout make_layout(int S, int N, int NG) {
   L.rScal = L.rPart + 2 * NG;
   L.rows = L.rScal + kNScal;
   return L;
-}
-
-// NASA-7 polynomials (src/zerork/nasa_poly.cpp:50-172), one species, one T.
-__device__ __forceinline__ void nasa_cp_h_g(const double *__restrict__ c, double T, double logT,
-                                            double *cp, double *h, double *g) {
-  const double invT = 1.0 / T;
-  const double m0 = T * 0.50000000000000000000;
-  const double T2 = T * T, T3 = T * T2, T4 = T * T3;
-  const double m1 = T2 * 0.33333333333333333333;
-  const double m2 = T3 * 0.25000000000000000000;
-  const double m3 = T4 * 0.20000000000000000000;
-  const double g0 = 1.0 - logT;
-  const double g1 = T * -0.50000000000000000000;
-  const double g2 = T2 * -0.16666666666666666667;
-  const double g3 = T3 * -0.08333333333333333333;
-  const double g4 = T4 * -0.05000000000000000000;
-  const int o = (T < c[0]) ? 1 : 8;
-  const double a1 = c[o], a2 = c[o + 1], a3 = c[o + 2], a4 = c[o + 3], a5 = c[o + 4],
-               a6 = c[o + 5], a7 = c[o + 6];
-  *cp = a1 + T * (a2 + T * (a3 + T * (a4 + T * a5)));
-  *h = a1 + a2 * m0 + a3 * m1 + a4 * m2 + a5 * m3 + a6 * invT;
-  *g = a1 * g0 + a2 * g1 + a3 * g2 + a4 * g3 + a5 * g4 + a6 * invT - a7;
-}
-
-__device__ __forceinline__ double nasa_cp(const double *__restrict__ c, double T) {
-  const int o = (T < c[0]) ? 1 : 8;
-  return c[o] + T * (c[o + 1] + T * (c[o + 2] + T * (c[o + 3] + T * c[o + 4])));
-}
-
-// One reaction (both steps) for the V states a thread owns (states
-// q + k*GS of the tile): rate constants, third body, falloff, step limiter
-// and concentration products.  The V independent chains give the scheduler
-// instruction-level parallelism across states.
-template <int TS, int V>
-__device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R, int q,
-                                              const double *__restrict__ sC,
-                                              const double *__restrict__ sG, double *sROP,
-                                              const double *T, const double *logT,
-                                              const double *invT, const double *lprt,
-                                              const double *Csum, double lim) {
-  constexpr int GS = TS / V;
-  double kf[V], kr[V];
-#pragma unroll
-  for (int k = 0; k < V; ++k) kf[k] = exp(R.lnA + R.n * logT[k] - R.Ta * invT[k]);
-  if (R.flags & kRevArr) {
-#pragma unroll
-    for (int k = 0; k < V; ++k) kr[k] = exp(R.lnA_r + R.n_r * logT[k] - R.Ta_r * invT[k]);
-  } else if (R.flags & kRevKeq) {
-    double s[V];
-#pragma unroll
-    for (int k = 0; k < V; ++k) s[k] = 0.0;
-    for (int i = 0; i < R.np; ++i) {
-      const double *gp = sG + R.p[i] * TS + q;
-#pragma unroll
-      for (int k = 0; k < V; ++k) s[k] += gp[k * GS];
-    }
-    for (int i = 0; i < R.nr; ++i) {
-      const double *gr = sG + R.r[i] * TS + q;
-#pragma unroll
-      for (int k = 0; k < V; ++k) s[k] -= gr[k * GS];
-    }
-#pragma unroll
-    for (int k = 0; k < V; ++k) kr[k] = exp(s[k] - R.lnA_r * lprt[k]) * kf[k];
-  } else {
-#pragma unroll
-    for (int k = 0; k < V; ++k) kr[k] = 0.0;
-  }
-  if (R.flags & kThirdBody) {
-    double Cm[V];
-#pragma unroll
-    for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
-    for (int e = m.tb_ptr[R.aux]; e < m.tb_ptr[R.aux + 1]; ++e) {
-      const double a = m.tb_alpha[e];
-      const double *cp = sC + m.tb_spc[e] * TS + q;
-#pragma unroll
-      for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
-    }
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-      kf[k] *= Cm[k];
-      kr[k] *= Cm[k];
-    }
-  }
-  if (R.flags & kFalloff) {
-    const int f = R.aux;
-    const double *p = m.fo_par + 8 * f;
-    const int fs = m.fo_spc[f];
-    const int ty = m.fo_type[f];
-    double Cm[V];
-    if (fs >= 0) {
-#pragma unroll
-      for (int k = 0; k < V; ++k) Cm[k] = sC[fs * TS + q + k * GS];
-    } else {
-#pragma unroll
-      for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
-      for (int e = m.fo_ptr[f]; e < m.fo_ptr[f + 1]; ++e) {
-        const double a = m.fo_alpha[e];
-        const double *cp = sC + m.fo_spc_eff[e] * TS + q;
-#pragma unroll
-        for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-      const double Klow = exp(p[0] + p[1] * logT[k] - p[2] * invT[k]);
-      double Pr = Klow * Cm[k] / kf[k];
-      if (Pr < 1.0e-300) Pr = 1.0e-300;
-      double lPr = log10(Pr);
-      double fT = 1.0;
-      if (ty == kTroe3 || ty == kTroe4) {
-        double Fc = 0.0;
-        if (p[4] != 0) Fc += (1.0 - p[3]) * exp(-T[k] / p[4]);
-        if (p[5] != 0) Fc += p[3] * exp(-T[k] / p[5]);
-        if (ty == kTroe4) Fc += exp(-p[6] * invT[k]);
-        if (Fc < 1.0e-300) Fc = 1.0e-300;
-        fT = log10(Fc);
-        const double nT = 0.75 - 1.27 * fT;
-        lPr -= (0.4 + 0.67 * fT);
-        lPr = lPr / (nT - 0.14 * lPr);
-        lPr *= lPr;
-        fT /= (1.0 + lPr);
-        fT = pow(10.0, fT);
-      } else if (ty == kSRI) {
-        const double xp = 1.0 / (1.0 + lPr * lPr);
-        fT = p[3] * exp(-p[4] * invT[k]);
-        if (p[5] > 0) fT += exp(-T[k] * p[5]);
-        fT = pow(fT, xp);
-        fT *= p[6];
-        fT *= pow(T[k], p[7]);
-      }
-      const double Pc = fT * Pr / (1.0 + Pr);
-      kf[k] *= Pc;
-      kr[k] *= Pc;
-    }
-  }
-  if (0.0 < lim && lim < 1.0e300) {
-#pragma unroll
-    for (int k = 0; k < V; ++k) {
-      kf[k] *= lim / (lim + kf[k]);
-      if (R.rev >= 0) kr[k] *= lim / (lim + kr[k]);
-    }
-  }
-  for (int i = 0; i < R.nr; ++i) {
-    const double *cp = sC + R.r[i] * TS + q;
-#pragma unroll
-    for (int k = 0; k < V; ++k) kf[k] *= cp[k * GS];
-  }
-#pragma unroll
-  for (int k = 0; k < V; ++k) sROP[R.fwd * TS + q + k * GS] = kf[k];
-  if (R.rev >= 0) {
-    for (int i = 0; i < R.np; ++i) {
-      const double *cp = sC + R.p[i] * TS + q;
-#pragma unroll
-      for (int k = 0; k < V; ++k) kr[k] *= cp[k * GS];
-    }
-#pragma unroll
-    for (int k = 0; k < V; ++k) sROP[R.rev * TS + q + k * GS] = kr[k];
-  }
-}
-
-__device__ __forceinline__ double clampy(double y, double mmf) {
-  if (fabs(y) < mmf) return (y < 0.0) ? -mmf : mmf;
-  return y;
 }
 
 // Sum over the groups of a warp (lanes q, q+GS, ...) with shuffles; lanes
@@ -407,7 +245,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           const double *th = m.thermo + 16 * s;
           const double iw = m.inv_mw[s], riw = m.ru_inv_mw[s];
           FORV {
-            const double yc = clampy(yload(s, k), kp.mmf);
+            const double yc = clamp_mass_fraction(yload(s, k), kp.mmf);
             const double c = (1.0 / v[k]) * iw * yc;
             sX[s * TS + q + k * GS] = c;
             pc[k] += c;
@@ -480,7 +318,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         const double riw = m.ru_inv_mw[j];
         double t2[V], trow[V];
         FORV {
-          t2[k] = mwj / clampy(yload(j, k), kp.mmf) * v[k];
+          t2[k] = mwj / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
           trow[k] = 0.0;
         }
         const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;

@@ -1,0 +1,227 @@
+// solver.cpp -- see solver.h.
+#include "solver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+
+namespace zrk {
+namespace {
+
+void ck(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+size_t put(std::vector<unsigned char> &b, const std::vector<T> &v) {
+  size_t off = (b.size() + 255) & ~size_t(255);
+  b.resize(off + std::max<size_t>(v.size() * sizeof(T), 16), 0);
+  if (!v.empty()) std::memcpy(b.data() + off, v.data(), v.size() * sizeof(T));
+  return off;
+}
+
+}  // namespace
+
+ReactorSolver::ReactorSolver(const std::string &mech, const std::string &therm) {
+  tables_ = load_chemkin(mech, therm);
+  pat_ = build_jac_pattern(tables_);
+  lus_ = analyze_lu(pat_);
+  dm_ = std::make_unique<DeviceMechanism>(tables_, pat_);
+  std::vector<unsigned char> b;
+  size_t o_cp = put(b, lus_.col_ptr), o_ri = put(b, lus_.row_idx), o_dg = put(b, lus_.diag_pos),
+         o_ip = put(b, lus_.iperm), o_jl = put(b, lus_.jac_to_lu), o_do = put(b, lus_.diag_of_orig);
+  ck(cudaMalloc(&lu_blob_, b.size()), "cudaMalloc(LU tables)");
+  ck(cudaMemcpy(lu_blob_, b.data(), b.size(), cudaMemcpyHostToDevice), "cudaMemcpy(LU tables)");
+  auto P = [&](size_t off) { return (const int *)((const unsigned char *)lu_blob_ + off); };
+  lud_.n = lus_.n;
+  lud_.nnz = lus_.nnz;
+  lud_.col_ptr = P(o_cp);
+  lud_.row_idx = P(o_ri);
+  lud_.diag = P(o_dg);
+  lud_.iperm = P(o_ip);
+  lud_.jac_to_lu = P(o_jl);
+  lud_.diag_of_orig = P(o_do);
+  ck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+  ck(cudaEventCreate(&ev0_), "event");
+  ck(cudaEventCreate(&ev1_), "event");
+}
+
+ReactorSolver::~ReactorSolver() {
+  cudaFree(lu_blob_);
+  cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
+  cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_); cudaFree(drop_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+cudaError_t ReactorSolver::reserve(int n, bool fp32) {
+  if (n <= cap_ && fp32 == cap_fp32_) return cudaSuccess;
+  cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
+  cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_);
+  dT_ = dP_ = dY_ = dv_ = dstate_ = nullptr;
+  dlu_ = nullptr;
+  dstats_ = nullptr;
+  dorder_ = dhead_ = nullptr;
+  cap_ = 0;
+  const int cap = std::max(n, 32);
+  const size_t S = tables_.nsp;
+  const long st = integ_state_doubles(dm_->view(), lud_);
+  cudaError_t e;
+  if ((e = cudaMalloc(&dT_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dP_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dv_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dY_, cap * S * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dstate_, (size_t)cap * st * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dlu_, (size_t)cap * lud_.nnz * (fp32 ? sizeof(float) : sizeof(double)))) !=
+      cudaSuccess)
+    return e;
+  if ((e = cudaMalloc(&dstats_, cap * sizeof(ReactorStats))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dorder_, cap * sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dhead_, sizeof(int))) != cudaSuccess) return e;
+  cap_ = cap;
+  cap_fp32_ = fp32;
+  return cudaSuccess;
+}
+
+int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
+                         int stride, double *cost, double *gpu_time, double *temp_delta,
+                         double temp_threshold, std::vector<ReactorStats> *stats,
+                         SolveStatsTotals *tot) {
+  if (n <= 0) return 0;
+  const int S = tables_.nsp;
+  cudaError_t e = reserve(n, o.lu_fp32);
+  if (e != cudaSuccess) {
+    last_error = std::string("device allocation: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  std::vector<int> order(n);
+  std::iota(order.begin(), order.end(), 0);
+  if (o.sort_reactors && cost)  // longest previous cost first (work queue)
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return std::fabs(cost[a]) > std::fabs(cost[b]); });
+  std::vector<double> Y((size_t)n * S), T0(T, T + n);
+  for (int r = 0; r < n; ++r) std::memcpy(&Y[(size_t)r * S], mf + (size_t)r * stride, S * sizeof(double));
+  const DevMech &m = dm_->view();
+  // launch mapping: up to 12 warps per CTA (register bound), rates of
+  // progress in shared memory when they fit, else in an L2-resident scratch
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t kSmem = 227 * 1024;
+  bool rop_smem = integ_smem_per_warp(m, lud_, true) * 12 <= kSmem;
+  int W = o.warps_per_cta > 0 ? o.warps_per_cta : 12;
+  while (W > 1 && integ_smem_per_warp(m, lud_, rop_smem) * W > kSmem) --W;
+  if (!rop_smem && integ_smem_per_warp(m, lud_, false) * W > kSmem) {
+    last_error = "mechanism too large for the integrator's shared memory";
+    return -1;
+  }
+  const int ctas = sms;
+  if (!rop_smem) {
+    size_t need = (size_t)ctas * W * m.nstep * sizeof(double);
+    if (need > drop_bytes_) {
+      cudaFree(drop_);
+      drop_ = nullptr;
+      drop_bytes_ = 0;
+      if ((e = cudaMalloc(&drop_, need)) != cudaSuccess) {
+        last_error = "ROP scratch allocation";
+        return -1;
+      }
+      drop_bytes_ = need;
+    }
+  }
+  IntegOpts io;
+  io.rtol = o.rtol;
+  io.atol = o.atol;
+  io.max_dt = o.max_dt;
+  io.nlscoef = o.nlscoef;
+  io.max_steps = o.max_steps;
+  io.max_retries = std::max(1, o.max_retries);
+  io.retry_atol_factor = o.retry_atol;
+  io.retry_rtol_factor = o.retry_rtol;
+  io.Tref = o.Tref;
+  io.mmf = o.mmf;
+  io.lim = o.lim;
+  io.sqrt_ur = std::sqrt(2.2204460492503131e-16);
+  io.lu_fp32 = o.lu_fp32 ? 1 : 0;
+  IntegArgs a;
+  a.n_reactors = n;
+  a.order = dorder_;
+  a.queue_head = dhead_;
+  a.dt = dt;
+  a.T = dT_;
+  a.P = dP_;
+  a.Y = dY_;
+  a.v = dv_;
+  a.state = dstate_;
+  a.state_stride = integ_state_doubles(m, lud_);
+  a.lu = dlu_;
+  a.lu_stride = lud_.nnz;
+  a.stats = dstats_;
+  a.rop_scratch = drop_;
+  cudaStream_t s = stream_;
+  if ((e = cudaMemcpyAsync(dT_, T, n * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dP_, P, n * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dY_, Y.data(), Y.size() * sizeof(double), cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(dorder_, order.data(), n * sizeof(int), cudaMemcpyHostToDevice, s)) !=
+          cudaSuccess ||
+      (e = cudaMemsetAsync(dhead_, 0, sizeof(int), s)) != cudaSuccess) {
+    last_error = std::string("H2D: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  cudaEventRecord(ev0_, s);
+  e = launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s);
+  cudaEventRecord(ev1_, s);
+  if (e != cudaSuccess) {
+    last_error = std::string("integrate launch: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  std::vector<ReactorStats> st(n);
+  if ((e = cudaMemcpyAsync(T, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(P, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(Y.data(), dY_, Y.size() * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(st.data(), dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+    last_error = std::string("integration: ") + cudaGetErrorString(e);
+    return -1;
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  int nfail = 0;
+  for (int r = 0; r < n; ++r) {
+    const ReactorStats &q = st[r];
+    if (q.status == 0) {
+      std::memcpy(mf + (size_t)r * stride, &Y[(size_t)r * S], S * sizeof(double));
+      if (temp_delta) {
+        double d = T[r] - T0[r];
+        temp_delta[r] = (d < temp_threshold) ? 0.0 : d;
+      }
+    } else {
+      ++nfail;
+    }
+    if (cost) cost[r] = q.status == 0 ? q.nsteps : -(double)std::max(1, q.nsteps);
+    if (gpu_time) gpu_time[r] = ms * 1e-3 / n;
+  }
+  if (stats) *stats = st;
+  if (tot) {
+    *tot = SolveStatsTotals();
+    for (auto &q : st) {
+      tot->nsteps += q.nsteps;
+      tot->nrej += q.nrej;
+      tot->nnewt += q.nnewt;
+      tot->njac += q.njac;
+      tot->nlu += q.nlu;
+      tot->nrhs += q.nrhs;
+    }
+    tot->nfailed = nfail;
+    tot->kernel_ms = ms;
+  }
+  return nfail;
+}
+
+}  // namespace zrk

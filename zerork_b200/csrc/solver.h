@@ -1,0 +1,75 @@
+// solver.h -- host driver of the batched reactor integration.
+//
+// Mirrors what ZeroRKReactorManager::SolveReactors does per call
+// (applications/cfd_plugin/zerork_reactor_manager.cpp:835-1155): order the
+// reactors by the previous call's cost (sort_reactors), integrate every
+// reactor for dt, write back T, P, mass fractions, cost (steps), time and
+// temperature delta.  All reactors run on the GPU (no CPU fallback).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "devmech.h"
+#include "integrator.h"
+#include "mech.h"
+#include "sparse_lu.h"
+
+namespace zrk {
+
+struct SolveOptions {
+  double rtol = 1.0e-8, atol = 1.0e-20, max_dt = 0.05, nlscoef = 0.05;
+  int max_steps = 5000, max_retries = 5;
+  double retry_atol = 0.1, retry_rtol = 1.0;
+  double Tref = 1.0, mmf = 1.0e-30, lim = 1.0e22;
+  bool lu_fp32 = false;
+  bool sort_reactors = true;
+  int warps_per_cta = 0;  // 0 = automatic
+};
+
+struct SolveStatsTotals {
+  long nsteps = 0, nrej = 0, nnewt = 0, njac = 0, nlu = 0, nrhs = 0;
+  int nfailed = 0;
+  float kernel_ms = 0.f;
+};
+
+class ReactorSolver {
+ public:
+  ReactorSolver(const std::string &mech, const std::string &therm);
+  ~ReactorSolver();
+  int nsp() const { return tables_.nsp; }
+  const MechTables &tables() const { return tables_; }
+  const LUSymbolic &lu() const { return lus_; }
+  // Integrate n reactors (host arrays; mf reactor-major with stride >= nsp).
+  // cost/gpu_time/temp_delta may be null.  Returns the number of failed
+  // reactors (state left unchanged for those), or -1 on a CUDA error.
+  int solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
+            int stride, double *cost, double *gpu_time, double *temp_delta,
+            double temp_threshold, std::vector<ReactorStats> *stats, SolveStatsTotals *tot);
+  std::string last_error;
+
+ private:
+  cudaError_t reserve(int n, bool fp32);
+  MechTables tables_;
+  JacPattern pat_;
+  LUSymbolic lus_;
+  std::unique_ptr<DeviceMechanism> dm_;
+  void *lu_blob_ = nullptr;
+  LUDev lud_{};
+  // device buffers
+  int cap_ = 0;
+  bool cap_fp32_ = false;
+  double *dT_ = nullptr, *dP_ = nullptr, *dY_ = nullptr, *dv_ = nullptr, *dstate_ = nullptr;
+  void *dlu_ = nullptr;
+  ReactorStats *dstats_ = nullptr;
+  int *dorder_ = nullptr, *dhead_ = nullptr;
+  double *drop_ = nullptr;
+  size_t drop_bytes_ = 0;
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+};
+
+}  // namespace zrk

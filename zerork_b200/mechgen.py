@@ -8,9 +8,14 @@ public benchmark suite: every species, reaction and state is drawn from
 numpy's PCG64 generator with a recorded seed.
 
 Parameter distributions (per workload):
-  * Arrhenius high-pressure/elementary rates: A log-uniform on [1e8, 1e16]
-    (cm-mol-s units), n uniform on [-2, 3], Ea uniform on [0, 50] kcal/mol.
-  * Falloff low-pressure limit: A_low = A * 10**U(3, 8), same n/Ea laws;
+  * Arrhenius high-pressure/elementary rates: pre-exponential factor
+    log-uniform on [1e8, 1e16] (cm-mol-s units) referenced to 1000 K, i.e.
+    the file's A is A' / 1000**n so that A T**n equals A' at 1000 K; n uniform
+    on [-2, 3], Ea uniform on [0, 50] kcal/mol.  (Unreferenced, A = 1e16 with
+    n = 3 gives bimolecular rate constants ~1e26 cm^3/mol/s and net rates that
+    are pure rounding noise at rtol 1e-8.)
+  * Falloff low-pressure limit: A_low' = A' * 10**U(3, 8) referenced the same
+    way, same n/Ea laws;
     Troe alpha U(0.1, 0.9), T*** U(10, 500) K, T* U(500, 5000) K and, for
     half of them, T** U(1000, 10000) K.
   * Third-body efficiencies: 0-3 collision partners with efficiency U(0.5, 6).
@@ -338,9 +343,10 @@ def generate(spec: SynthSpec) -> SynthMechanism:
     lines += ["END", "REACTIONS CAL/MOLE MOLES"]
     colliders = [i for i in range(S)]
     for idx, (r, p, kind) in enumerate(chosen):
-        A = 10 ** rng.uniform(8.0, 16.0)
+        Aref = 10 ** rng.uniform(8.0, 16.0)
         n = rng.uniform(-2.0, 3.0)
         Ea = rng.uniform(0.0, 50000.0)
+        A = Aref / 1000.0 ** n
         lhs = " + ".join(names[i] for i in r)
         rhs = " + ".join(names[i] for i in p)
         arrow = " => " if idx in irrev else " <=> "
@@ -352,8 +358,8 @@ def generate(spec: SynthSpec) -> SynthMechanism:
             eq = f"{lhs}{arrow}{rhs}"
         lines.append(f"{eq:<48s} {A:12.5E} {n:8.4f} {Ea:12.3f}")
         if kind == "fo":
-            Al = A * 10 ** rng.uniform(3.0, 8.0)
             nl = rng.uniform(-2.0, 3.0)
+            Al = Aref * 10 ** rng.uniform(3.0, 8.0) / 1000.0 ** nl
             El = rng.uniform(0.0, 50000.0)
             lines.append(f"   LOW / {Al:12.5E} {nl:8.4f} {El:12.3f} /")
             if idx in troe:
