@@ -24,6 +24,7 @@
 #define NEWTON_MAXITER 3
 #define MIN_FACTOR 0.2
 #define MAX_FACTOR 10.0
+#define ETA_KEEP 1.5
 
 static const double KAPPA[MAXO + 1] = {0.0, -0.1850, -1.0 / 9.0, -0.0823, -0.0415, 0.0};
 
@@ -318,6 +319,8 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
     if (fp > best) { best = fp; dq = 1; }
     q += dq;
     double fac = fmin(MAX_FACTOR, safety * best);
+    /* CVODE's step-size hysteresis (eta < 1.5 keeps h): fewer matrix updates */
+    if (fac < ETA_KEEP) fac = 1.0;
     change_D(b, q, fac);
     h *= fac;
     neq = 0;

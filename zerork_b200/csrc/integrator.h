@@ -57,6 +57,14 @@ struct IntegArgs {
 };
 
 size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);
+// CTA-per-reactor dense-block integrator (integrator_dense.cu); IntegArgs.state
+// holds the per-reactor Jacobian (state_stride = Jacobian nonzeros).
+// spill: bit 1 puts rates of progress, bit 2 the BDF differences, in a global
+// slice of IntegArgs.rop_scratch per CTA (dense_spill_doubles each).
+size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill);
+size_t dense_spill_doubles(const DevMech &m);
+cudaError_t launch_integrate_dense(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                   int threads, int ctas, int spill, cudaStream_t stream);
 long integ_state_doubles(const DevMech &m, const LUDev &lu);
 cudaError_t launch_integrate(const DevMech &m, const LUDev &lu, const IntegOpts &o,
                              const IntegArgs &a, int warps_per_cta, int ctas, bool rop_in_smem,

@@ -77,6 +77,8 @@ void set_defaults(zerork_handle_impl *h) {
   I["n_reactors_max"] = 1024;
   I["lu_fp32"] = 0;
   I["gpu_warps_per_cta"] = 0;
+  I["gpu_method"] = 0;
+  I["gpu_threads"] = 0;
 }
 
 std::string trim(const std::string &s) {
@@ -207,6 +209,8 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
   o.lu_fp32 = I["lu_fp32"] != 0;
   o.sort_reactors = I["sort_reactors"] != 0;
   o.warps_per_cta = I["gpu_warps_per_cta"];
+  o.method = I["gpu_method"];
+  o.threads = I["gpu_threads"];
   // aux fields owned by the handle when the caller gave none
   // (zerork_reactor_manager.cpp:502-519)
   const int n = n_reactors;

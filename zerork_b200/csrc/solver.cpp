@@ -105,6 +105,21 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   std::vector<double> Y((size_t)n * S), T0(T, T + n);
   for (int r = 0; r < n; ++r) std::memcpy(&Y[(size_t)r * S], mf + (size_t)r * stride, S * sizeof(double));
   const DevMech &m = dm_->view();
+  const size_t kSmemMax = 227 * 1024;
+  // dense block in shared memory, spilling the rates of progress and then the
+  // BDF differences to an L2-resident global slice if needed
+  int spill = -1;
+  for (int sp : {0, 1, 3})
+    if (dense_smem_bytes(m, o.lu_fp32, nullptr, sp) <= kSmemMax) {
+      spill = sp;
+      break;
+    }
+  int method = o.method;
+  if (method == 0) method = spill >= 0 ? 1 : 2;
+  if (method == 1 && spill < 0) {
+    last_error = "dense block does not fit in shared memory";
+    return -1;
+  }
   // launch mapping: up to 12 warps per CTA (register bound), rates of
   // progress in shared memory when they fit, else in an L2-resident scratch
   int dev = 0, sms = 148;
@@ -119,8 +134,22 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     return -1;
   }
   const int ctas = sms;
-  if (!rop_smem) {
-    size_t need = (size_t)ctas * W * m.nstep * sizeof(double);
+  int dthreads = o.threads;
+  int dctas = ctas;
+  if (method == 1) {
+    if (dthreads <= 0) {
+      const int work = std::max(m.nsp + 1, m.nrxn / 2);
+      dthreads = 32;
+      while (dthreads < work && dthreads < 512) dthreads *= 2;
+    }
+    const size_t sm = dense_smem_bytes(m, o.lu_fp32, nullptr, spill);
+    int per_sm = (int)std::min<size_t>(kSmemMax / sm, (size_t)(2048 / dthreads));
+    per_sm = std::max(1, std::min(per_sm, 65536 / (dthreads * 128)));
+    dctas = std::min(n, sms * per_sm);
+  }
+  if (!rop_smem || (method == 1 && spill > 0)) {
+    size_t need = method == 1 ? (size_t)dctas * dense_spill_doubles(m) * sizeof(double)
+                              : (size_t)ctas * W * m.nstep * sizeof(double);
     if (need > drop_bytes_) {
       cudaFree(drop_);
       drop_ = nullptr;
@@ -172,8 +201,13 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     last_error = std::string("H2D: ") + cudaGetErrorString(e);
     return -1;
   }
+  if (method == 1) {
+    a.state = dstate_;
+    a.state_stride = m.nnz;
+  }
   cudaEventRecord(ev0_, s);
-  e = launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s);
+  e = method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)
+                  : launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s);
   cudaEventRecord(ev1_, s);
   if (e != cudaSuccess) {
     last_error = std::string("integrate launch: ") + cudaGetErrorString(e);
@@ -220,6 +254,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     }
     tot->nfailed = nfail;
     tot->kernel_ms = ms;
+    tot->method = method;
   }
   return nfail;
 }

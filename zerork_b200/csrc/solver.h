@@ -28,12 +28,15 @@ struct SolveOptions {
   bool lu_fp32 = false;
   bool sort_reactors = true;
   int warps_per_cta = 0;  // 0 = automatic
+  int method = 0;         // 0 automatic, 1 CTA dense block, 2 warp sparse LU
+  int threads = 0;        // CTA size of the dense method (0 = automatic)
 };
 
 struct SolveStatsTotals {
   long nsteps = 0, nrej = 0, nnewt = 0, njac = 0, nlu = 0, nrhs = 0;
   int nfailed = 0;
   float kernel_ms = 0.f;
+  int method = 0;
 };
 
 class ReactorSolver {
