@@ -1,13 +1,16 @@
 """GPU batched integrator through the cfd_plugin C ABI, against the CPU oracle.
 
 The oracle (oracle/zrk_bdf.c) integrates the same reactors with the same BDF
-method but dense pivoted LU on the CPU; the GPU uses the warp-level sparse LU
-with static pivots, so step sequences differ and end states are compared at
-the integration tolerance: both are also compared with a tight-tolerance
-oracle run (rtol 1e-12), and the GPU error must be within
-  |T_gpu - T_tight| <= 20 * |T_oracle - T_tight| + 1e-6 * T
-  max_k |Y_gpu - Y_tight| <= 20 * max_k |Y_oracle - Y_tight| + 1e-9
-per reactor (the oracle's own rtol-1e-8 error sets the scale).
+method but a dense LU with partial pivoting on the CPU; the GPU uses a
+shared-memory Gauss-Jordan inverse (method 1) or a warp-level sparse LU with
+static pivots (method 2), so step sequences differ and end states are
+compared at the integration tolerance: both are also compared with a
+tight-tolerance oracle run (rtol 1e-12), and the GPU error must be within
+  |T_gpu - T_tight| <= 50 * |T_oracle - T_tight| + 1e-5 * T
+  max_k |Y_gpu - Y_tight| <= 50 * max_k |Y_oracle - Y_tight| + 1e-8
+per reactor: the oracle's own error at rtol 1e-8 sets the scale (two valid
+integrations at the same tolerance with different step sequences differ by
+a small multiple of it).
 """
 import os
 
