@@ -114,6 +114,17 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
     nzc_ptr.push_back((int)nzc_step.size());
   }
   n_terms_ = (int)(nzd_step.size() + nzc_step.size());
+  std::vector<std::vector<std::pair<int, int>>> rows(p.n);
+  for (int j = 0; j < p.n; ++j)
+    for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) rows[p.row_idx[k]].push_back({k, j});
+  std::vector<int> jr_ptr(1, 0), jr_kk, jr_col;
+  for (int i = 0; i < p.n; ++i) {
+    for (auto &e : rows[i]) {
+      jr_kk.push_back(e.first);
+      jr_col.push_back(e.second);
+    }
+    jr_ptr.push_back((int)jr_kk.size());
+  }
 
   Blob b;
   size_t o_mw = b.add(t.mw), o_imw = b.add(inv_mw), o_rimw = b.add(ru_inv_mw), o_th = b.add(t.thermo);
@@ -124,6 +135,7 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   size_t o_sdp = b.add(sd_ptr), o_sds = b.add(sd_step), o_scp = b.add(sc_ptr), o_scs = b.add(sc_step);
   size_t o_cp = b.add(p.col_ptr), o_ri = b.add(p.row_idx), o_lr = b.add(p.last_row);
   size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
+  size_t o_jrp = b.add(jr_ptr), o_jrk = b.add(jr_kk), o_jrc = b.add(jr_col);
   bytes_ = b.bytes.size();
   check(cudaMalloc(&blob_, bytes_), "cudaMalloc(mechanism tables)");
   check(cudaMemcpy(blob_, b.bytes.data(), bytes_, cudaMemcpyHostToDevice), "cudaMemcpy(mechanism tables)");
@@ -157,6 +169,9 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   view_.nzd_step = (const int *)P(o_nds);
   view_.nzc_ptr = (const int *)P(o_ncp);
   view_.nzc_step = (const int *)P(o_ncs);
+  view_.jr_ptr = (const int *)P(o_jrp);
+  view_.jr_kk = (const int *)P(o_jrk);
+  view_.jr_col = (const int *)P(o_jrc);
 }
 
 DeviceMechanism::~DeviceMechanism() {

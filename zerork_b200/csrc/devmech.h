@@ -50,6 +50,10 @@ struct DevMech {
   // Jacobian pattern and per-nonzero gather lists
   const int *col_ptr, *row_idx, *last_row;
   const int *nzd_ptr, *nzd_step, *nzc_ptr, *nzc_step;
+  // row-wise view of the Jacobian pattern: row i has entries jr_kk[p] (index
+  // into the compressed-column values) in columns jr_col[p], p in
+  // [jr_ptr[i], jr_ptr[i+1])
+  const int *jr_ptr, *jr_kk, *jr_col;
 };
 
 // Host-side builder; owns the device allocation.

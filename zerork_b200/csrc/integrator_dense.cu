@@ -204,12 +204,21 @@ __device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, doub
     __syncthreads();
     for (int j = tid; j < n; j += nt) A[k * lda + j] = (j == k ? (LT)1 : A[k * lda + j]) * pinv;
     __syncthreads();
-    for (int e = tid; e < n * n; e += nt) {
-      const int i = e / n, j = e - i * n;
-      if (i == k) continue;
-      const LT f = colk[i];
-      const LT a = (j == k) ? (LT)0 : A[i * lda + j];
-      A[i * lda + j] = a - f * A[k * lda + j];
+    // rank-1 update: warp w owns rows i = w (mod warps), lane l the columns
+    // j = l (mod 32); rows whose multiplier is zero (untouched by the fill
+    // so far) are skipped whole.
+    {
+      const int lane = tid & 31, nw = nt >> 5;
+      const LT *Ak = A + k * lda;
+      for (int i = tid >> 5; i < n; i += nw) {
+        const LT f = colk[i];
+        if (i == k || f == (LT)0) continue;
+        LT *Ai = A + i * lda;
+        for (int j = lane; j < n; j += 32) {
+          const LT a = (j == k) ? (LT)0 : Ai[j];
+          Ai[j] = a - f * Ak[j];
+        }
+      }
     }
     __syncthreads();
   }
@@ -384,6 +393,20 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         for (int i = tid; i < n; i += nt) s.tmp[i] = c * s.f[i] - s.psi[i] - s.d[i];
         __syncthreads();
         apply_inverse<LT>(s, n, lda, s.tmp, s.yp);
+        if constexpr (sizeof(LT) == sizeof(float)) {
+          // one step of iterative refinement with the residual of the FP64
+          // Newton matrix (I - c_lu J) taken row-wise from the sparse J, so
+          // the single-precision inverse only has to be a contraction
+          for (int i = tid; i < n; i += nt) {
+            double jx = 0.0;
+            for (int p = m.jr_ptr[i]; p < m.jr_ptr[i + 1]; ++p) jx += J[m.jr_kk[p]] * s.yp[m.jr_col[p]];
+            s.colk[i] = s.tmp[i] - (s.yp[i] - c_lu * jx);
+          }
+          __syncthreads();
+          apply_inverse<LT>(s, n, lda, s.colk, s.tmp);
+          for (int i = tid; i < n; i += nt) s.yp[i] += s.tmp[i];
+          __syncthreads();
+        }
         double a = 0.0;
         for (int i = tid; i < n; i += nt) {
           const double dy = s.yp[i] * gscale;
