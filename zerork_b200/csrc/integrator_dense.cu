@@ -32,6 +32,8 @@ struct Smem {
   void *A;      // n x lda inverse (LT)
   int *piv;     // n
   double *colk; // n (LT-sized use)
+  double *wlu;  // n: error-weight scale the stored inverse was formed with
+  double *bs;   // n: scaled right-hand side
 };
 
 // Sum over the CTA; every thread gets thread 0's total (deterministic).
@@ -145,18 +147,28 @@ __device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
   return 0;
 }
 
-// A <- (I - cJ)^{-1}, Gauss-Jordan with partial pivoting in shared memory.
-// Returns nonzero (all threads) for a singular or non-finite matrix.
+// A <- (W (I - cJ) W^-1)^{-1} with W = diag(1/scale) the error weights of
+// the current step (scale = atol + rtol |y|): the similarity transform turns
+// J_ij into J_ij scale_j / scale_i, the Jacobian of relative changes, which
+// is far better balanced than J for species spanning 20 decades of mass
+// fraction and keeps the single-precision inverse accurate in the weighted
+// norm the Newton test uses.  Gauss-Jordan with partial pivoting in shared
+// memory.  Returns nonzero (all threads) for a singular or non-finite matrix.
 template <class LT>
 __device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda) {
   LT *A = (LT *)s.A;
   LT *colk = (LT *)s.colk;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int i = tid; i < n * lda; i += nt) A[i] = (LT)0;
+  for (int i = tid; i < n; i += nt) s.wlu[i] = s.scale[i];
   __syncthreads();
-  for (int j = 0; j < n; ++j)  // Jacobian column j: scatter rows
-    for (int kk = m.col_ptr[j] + tid; kk < m.col_ptr[j + 1]; kk += nt)
-      A[m.row_idx[kk] * lda + j] = (LT)(-c * J[kk]);
+  for (int i = tid; i < n; i += nt) {  // Jacobian row i from the row-wise view
+    const double ci = -c / s.wlu[i];
+    for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) {
+      const int j = m.jr_col[q];
+      A[i * lda + j] = (LT)(ci * J[m.jr_kk[q]] * s.wlu[j]);
+    }
+  }
   __syncthreads();
   for (int i = tid; i < n; i += nt) A[i * lda + i] += (LT)1;
   __syncthreads();
@@ -281,15 +293,17 @@ __device__ void make_consts(Consts &b) {
   }
 }
 
-// x = A b (A the stored inverse), into x (shared).
+// x = (I - c_lu J)^{-1} b = W^-1 A W b (A the stored inverse), into x (shared).
 template <class LT>
 __device__ void apply_inverse(const Smem &s, int n, int lda, const double *b, double *x) {
   const LT *A = (const LT *)s.A;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s.bs[i] = b[i] / s.wlu[i];
+  __syncthreads();
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double acc = 0.0;
     const LT *row = A + (size_t)i * lda;
-    for (int j = 0; j < n; ++j) acc += (double)row[j] * b[j];
-    x[i] = acc;
+    for (int j = 0; j < n; ++j) acc += (double)row[j] * s.bs[j];
+    x[i] = acc * s.wlu[i];
   }
   __syncthreads();
 }
@@ -535,6 +549,8 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
   s.tmp = p; p += n;
   s.yp = p; p += n;
   s.colk = p; p += n;
+  s.wlu = p; p += n;
+  s.bs = p; p += n;
   s.piv = (int *)p; p += (n + 1) / 2 + 1;
   s.A = p;
   Consts bc;
@@ -596,7 +612,7 @@ size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill) {
   const int n = m.nsp + 1;
   const int lda = (n % 2 == 1) ? n : n + 1;  // odd row stride: conflict-free column walks
   if (lda_out) *lda_out = lda;
-  size_t d = 72 + 3 * (size_t)m.nsp + 10 * (size_t)n + ((n + 1) / 2 + 1);
+  size_t d = 72 + 3 * (size_t)m.nsp + 12 * (size_t)n + ((n + 1) / 2 + 1);
   if (!(spill & 1)) d += m.nstep;
   if (!(spill & 2)) d += (kMaxOrder + 3) * (size_t)n;
   size_t bytes = d * sizeof(double) + (size_t)n * lda * (fp32 ? sizeof(float) : sizeof(double));
