@@ -99,6 +99,29 @@ int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double
 int zrk_rates_jac_dev(zrk_mech_t m, int n, int ld, const double *T, const double *P,
                       const double *Y, double *wdot, double *jac, double *ydot, void *stream);
 
+/* No counterpart in the reference.  zrk_rates_jac_dev for callers that
+ * cannot have the library allocate device memory during a call: codes whose
+ * own pool allocator owns the GPU's memory after start-up, code running
+ * where a cudaMalloc would synchronize the device, or hosts whose device
+ * footprint must stay fixed after set-up.  Same arguments, kernel and
+ * results as zrk_rates_jac_dev, with the kernel's global-workspace mapping
+ * (the handle's tile size, states per thread and warps) always used and its
+ * workspace taken from a fixed array of ZRK_NOALLOC_SCRATCH_BYTES inside the
+ * library, which every device that loads the library holds until the
+ * process exits; the grid is cut to the tiles that fit in it.  Returns
+ * ZRK_ERR_INVALID_ARGUMENT, with the sizes in zrk_last_error(), when one
+ * tile's workspace alone is larger than the array.  The first call on a
+ * device looks the array's device address up (cudaGetSymbolAddress) and
+ * caches it: make that first call before capturing any stream.  The kernel
+ * writes every workspace word before reading it, so the array needs no
+ * clearing, but all calls in the process share it: calls that overlap on
+ * the GPU (different streams or handles without ordering between them)
+ * race and give wrong results. */
+#define ZRK_NOALLOC_SCRATCH_BYTES (8u << 20)
+int zrk_rates_jac_dev_noalloc(zrk_mech_t m, int n, int ld, const double *T, const double *P,
+                              const double *Y, double *wdot, double *jac, double *ydot,
+                              void *stream);
+
 /* Same with host buffers (species-major, ld = n): copies in, computes,
  * copies out, synchronizes.  Host buffers may be pageable or pinned. */
 int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, const double *Y,
