@@ -39,6 +39,9 @@ void zo_bdf_default_opts(zo_bdf_opts *o) {
   o->min_mass_frac = 1.0e-30;
   o->step_limiter = 1.0e22;
   o->analytic = 1;
+  o->max_retries = 5;
+  o->retry_atol = 0.1;
+  o->retry_rtol = 1.0;
 }
 
 typedef struct {
@@ -188,11 +191,15 @@ static void change_D(bdf_t *b, int order, double fac) {
   memcpy(b->D, Dn, sizeof(double) * (order + 1) * n);
 }
 
-static int integrate(bdf_t *b, double *y0, double t_end) {
+/* One attempt (one CVodeReInit..failure span): integrates y0 over
+ * [0, t_end].  On failure y0 receives the last accepted state and *t_done
+ * the time it was reached (D[0], which step-size changes leave unchanged). */
+static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double atol, double *t_done) {
   const int n = b->n;
   const zo_bdf_opts *o = b->o;
-  const double rtol = o->rtol, atol = o->atol;
   double t = 0.0;
+  int rc = 0, nsteps_att = 0;
+  *t_done = 0.0;
   memcpy(b->y, y0, sizeof(double) * n);
   if (rhs(b, b->y, b->f0)) return -1;
   /* initial step: Hairer-Norsett-Wanner estimate (first order) */
@@ -214,10 +221,10 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
   memset(b->D, 0, sizeof(double) * (MAXO + 3) * n);
   memcpy(b->D, b->y, sizeof(double) * n);
   for (int i = 0; i < n; ++i) b->D[n + i] = b->f0[i] * h;
-  if (take_jacobian(b, b->y, b->f0)) return -2;
-  if (factor(b, h / b->alp[q])) return -3;
+  if (take_jacobian(b, b->y, b->f0)) { rc = -2; goto failed; }
+  if (factor(b, h / b->alp[q])) { rc = -3; goto failed; }
   while (t < t_end) {
-    if (b->st.nsteps >= o->max_steps) return -4;
+    if (nsteps_att >= o->max_steps) { rc = -4; goto failed; }
     int accepted = 0;
     double safety = 0.9, err_norm = 0.0;
     while (!accepted) {
@@ -227,7 +234,7 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
         change_D(b, q, fac);
         h = t_end - t;
       }
-      if (!(t + h > t)) return -5; /* no progress (or h not finite) */
+      if (!(t + h > t)) { rc = -5; goto failed; } /* no progress (or h not finite) */
       const double t_new = t + h;
       for (int i = 0; i < n; ++i) {
         double s = 0.0;
@@ -240,7 +247,7 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
       }
       const double c = h / b->alp[q];
       if (fabs(c / b->c_lu - 1.0) > 0.3)
-        if (factor(b, c)) return -3;
+        if (factor(b, c)) { rc = -3; goto failed; }
       /* modified Newton, CVODE-style convergence test (Hindmarsh et al.,
        * ACM TOMS 31 (2005) 363-396, sec. 2.1): rate estimate carried across
        * steps, converged when econ * |delta| * min(1, rate) <= nlscoef,
@@ -266,9 +273,9 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
       }
       if (!conv) {
         if (!b->jac_current) {
-          if (rhs(b, b->ypred, b->f0)) return -6;
-          if (take_jacobian(b, b->ypred, b->f0)) return -2;
-          if (factor(b, c)) return -3;
+          if (rhs(b, b->ypred, b->f0)) { rc = -6; goto failed; }
+          if (take_jacobian(b, b->ypred, b->f0)) { rc = -2; goto failed; }
+          if (factor(b, c)) { rc = -3; goto failed; }
           continue;
         }
         change_D(b, q, 0.5);
@@ -279,7 +286,7 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
       safety = 0.9 * (2 * NEWTON_MAXITER + 1) / (2.0 * NEWTON_MAXITER + it);
       for (int i = 0; i < n; ++i) b->err[i] = b->econ[q] * b->d[i];
       err_norm = rms(b->err, b->scale, n);
-      if (!isfinite(err_norm)) return -7;
+      if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
         double fac = fmax(MIN_FACTOR, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D(b, q, fac);
@@ -291,6 +298,7 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
       t = t_new;
     }
     b->st.nsteps++;
+    nsteps_att++;
     neq++;
     b->jac_current = 0;
     /* update differences */
@@ -326,7 +334,12 @@ static int integrate(bdf_t *b, double *y0, double t_end) {
     neq = 0;
   }
   memcpy(y0, b->D, sizeof(double) * n); /* D[0] holds y at t_end */
+  *t_done = t;
   return 0;
+failed:
+  memcpy(y0, b->D, sizeof(double) * n);
+  *t_done = t;
+  return rc;
 }
 
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
@@ -361,7 +374,25 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   zo_reactor_set_density(b.r, *T, *P, Y);
   for (int j = 0; j < ns; ++j) y[j] = Y[j];
   y[ns] = *T / o->Tref;
-  int rc = integrate(&b, y, dt);
+  /* retry loop, solver_cvode.cpp:227-246: a failed attempt restarts the
+   * method (order 1, new initial step) from the last accepted state with
+   * adjusted tolerances; max_steps counts per attempt, as CVodeReInit
+   * resets CVODE's step counter */
+  double *ystart = (double *)calloc(n, sizeof(double));
+  memcpy(ystart, y, sizeof(double) * n);
+  double rtol = o->rtol, atol = o->atol, t_left = dt;
+  int rc = 0;
+  for (int attempt = 0;; ++attempt) {
+    double t_done = 0.0;
+    rc = integrate(&b, y, t_left, rtol, atol, &t_done);
+    if (rc == 0 || attempt + 1 >= o->max_retries) break;
+    b.st.retries++;
+    t_left -= t_done;
+    atol *= o->retry_atol;
+    rtol *= o->retry_rtol;
+  }
+  if (rc != 0) memcpy(y, ystart, sizeof(double) * n);
+  free(ystart);
   b.st.status = rc;
   if (rc == 0) {
     *T = y[ns] * o->Tref;

@@ -57,11 +57,13 @@ class ZoBdfOpts(C.Structure):
     _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("max_dt", C.c_double),
                 ("nlscoef", C.c_double), ("max_steps", C.c_int), ("Tref", C.c_double),
                 ("min_mass_frac", C.c_double), ("step_limiter", C.c_double),
-                ("analytic", C.c_int)]
+                ("analytic", C.c_int), ("max_retries", C.c_int), ("retry_atol", C.c_double),
+                ("retry_rtol", C.c_double)]
 
 
 class ZoBdfStats(C.Structure):
-    _fields_ = [(n, C.c_int) for n in ("nsteps", "nrej", "nnewt", "njac", "nlu", "nrhs", "status")]
+    _fields_ = [(n, C.c_int) for n in ("nsteps", "nrej", "nnewt", "njac", "nlu", "nrhs", "status",
+                                           "retries")]
 
 
 # array name -> (dtype, size expression over the struct's counts)

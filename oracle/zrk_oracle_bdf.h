@@ -30,10 +30,17 @@ typedef struct zo_bdf_opts {
   double Tref, min_mass_frac, step_limiter;
   int analytic; /* 1: SetupJacobianSparse values; 0: dense divided differences
                    (the plugin's analytic = 0, reactor_nvector_serial.cpp:360) */
+  /* cvode_num_retries and the tolerance adjustments: after a failed attempt
+   * the integration restarts from the last accepted state with atol *=
+   * retry_atol, rtol *= retry_rtol, at most max_retries attempts in all
+   * (solver_cvode.cpp:216-246) */
+  int max_retries;
+  double retry_atol, retry_rtol;
 } zo_bdf_opts;
 
 typedef struct zo_bdf_stats {
   int nsteps, nrej, nnewt, njac, nlu, nrhs, status; /* status 0 ok, <0 failure */
+  int retries;
 } zo_bdf_stats;
 
 void zo_bdf_default_opts(zo_bdf_opts *o);

@@ -21,6 +21,7 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kNewtonMaxIter = 3;
 constexpr double kMinFactor = 0.2;
 constexpr double kMaxFactor = 10.0;
+constexpr double kEtaKeep = 1.5;
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -249,15 +250,18 @@ __device__ __forceinline__ double wrms_scaled(const double *x, const double *s, 
 }
 
 // One integration attempt from t = 0 to t_end; y holds the start state and,
-// on return, the last accepted state.  Returns 0 or a negative failure code.
+// on return, the last accepted state, reached at t_done.  Returns 0 or a
+// negative failure code.
 template <class LT>
 __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o, const BdfConst &bc,
                            const Warp &w, const Vecs &V, LT *LU, double v, double t_end,
-                           double rtol, double atol, ReactorStats &st, int lane) {
+                           double rtol, double atol, ReactorStats &st, int lane, double &t_done) {
   const int n = m.nsp + 1;
   const int jnnz = m.nnz;
   LT *x = (LT *)w.X;
   double t = 0.0;
+  int rc = 0;
+  t_done = 0.0;
   // f0 = f(y0); initial step (Hairer-Norsett-Wanner)
   st.nrhs++;
   if (rhs_warp(m, o, w, v, V.y, V.f0, lane, false, nullptr)) return -1;
@@ -279,7 +283,8 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   double h = fmin(100.0 * h0, h1);
   h = fmin(h, o.max_dt);
   h = fmin(h, t_end);
-  int q = 1, neq = 0;
+  int q = 1, neq = 0, jac_current = 1, nsteps = 0;
+  double c_lu = h / bc.alp[q], crate = 1.0;
   for (int i = lane; i < (kMaxOrder + 3) * n; i += 32) V.D[i] = 0.0;
   __syncwarp();
   for (int i = lane; i < n; i += 32) {
@@ -288,15 +293,11 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   }
   __syncwarp();
   st.njac++;
-  if (jac_warp(m, o, w, v, V.y, V.f0, V.J, V.tmp, V.d, lane)) return -2;
-  int jac_current = 1;
-  double c_lu = h / bc.alp[q];
+  if (jac_warp(m, o, w, v, V.y, V.f0, V.J, V.tmp, V.d, lane)) { rc = -2; goto failed; }
   st.nlu++;
-  if (lu_factor_warp<LT>(lu, V.J, jnnz, c_lu, LU, x, lane)) return -3;
-  double crate = 1.0;
-  int nsteps = 0;
+  if (lu_factor_warp<LT>(lu, V.J, jnnz, c_lu, LU, x, lane)) { rc = -3; goto failed; }
   while (t < t_end) {
-    if (nsteps >= o.max_steps) return -4;
+    if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
     double safety = 0.9, err_norm = 0.0;
     while (!accepted) {
@@ -308,7 +309,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         change_D(V.D, n, q, (t_end - t) / h, lane);
         h = t_end - t;
       }
-      if (!(t + h > t)) return -5;  // no progress (or h not finite)
+      if (!(t + h > t)) { rc = -5; goto failed; }  // no progress (or h not finite)
       const double t_new = t + h;
       for (int i = lane; i < n; i += 32) {
         double s = 0.0, ps = 0.0;
@@ -326,7 +327,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         st.nlu++;
         c_lu = c;
         crate = 1.0;
-        if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) return -3;
+        if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) { rc = -3; goto failed; }
       }
       const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
       bool conv = false;
@@ -367,14 +368,14 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       if (!conv) {
         if (!jac_current) {
           st.nrhs++;
-          if (rhs_warp(m, o, w, v, V.ypred, V.f0, lane, false, nullptr)) return -6;
+          if (rhs_warp(m, o, w, v, V.ypred, V.f0, lane, false, nullptr)) { rc = -6; goto failed; }
           st.njac++;
-          if (jac_warp(m, o, w, v, V.ypred, V.f0, V.J, V.tmp, V.f, lane)) return -2;
+          if (jac_warp(m, o, w, v, V.ypred, V.f0, V.J, V.tmp, V.f, lane)) { rc = -2; goto failed; }
           jac_current = 1;
           st.nlu++;
           c_lu = c;
           crate = 1.0;
-          if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) return -3;
+          if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) { rc = -3; goto failed; }
           continue;
         }
         change_D(V.D, n, q, 0.5, lane);
@@ -389,7 +390,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         a += e * e;
       }
       err_norm = sqrt(wsum(a) / n);
-      if (!isfinite(err_norm)) return -7;
+      if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
         const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D(V.D, n, q, fac, lane);
@@ -437,14 +438,21 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
     if (fm > best) { best = fm; dq = -1; }
     if (fp > best) { best = fp; dq = 1; }
     q += dq;
-    const double fac = fmin(kMaxFactor, safety * best);
+    double fac = fmin(kMaxFactor, safety * best);
+    if (fac < kEtaKeep) fac = 1.0;  // CVODE's step-size hysteresis
     change_D(V.D, n, q, fac, lane);
     h *= fac;
     neq = 0;
   }
   for (int i = lane; i < n; i += 32) V.y[i] = V.D[i];
   __syncwarp();
+  t_done = t;
   return 0;
+failed:  // D[0] holds the last accepted state (step-size changes keep it)
+  for (int i = lane; i < n; i += 32) V.y[i] = V.D[i];
+  __syncwarp();
+  t_done = t;
+  return rc;
 }
 
 template <class LT>
@@ -502,9 +510,12 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
+    double t_left = a.dt;
     for (int attempt = 0;; ++attempt) {
-      rc = bdf_attempt<LT>(m, lu, o, bc, w, V, LU, v, a.dt, rtol, atol, rs, lane);
+      double t_done = 0.0;
+      rc = bdf_attempt<LT>(m, lu, o, bc, w, V, LU, v, t_left, rtol, atol, rs, lane, t_done);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
+      t_left -= t_done;
       // solver_cvode.cpp:236-246: adjust tolerances and start over from the
       // last accepted state for the remaining time
       rs.retries++;

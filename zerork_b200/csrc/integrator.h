@@ -34,6 +34,7 @@ struct IntegOpts {
   double retry_atol_factor, retry_rtol_factor;
   double Tref, mmf, lim, sqrt_ur;
   int lu_fp32;  // factor and apply the Newton matrix in FP32
+  double eps_lin;  // Krylov tolerance: eps_lin * nlscoef / error constant (WRMS)
 };
 
 // Per-reactor statistics written by the kernel.

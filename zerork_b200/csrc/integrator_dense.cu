@@ -24,6 +24,7 @@ constexpr int kNewtonMaxIter = 3;
 constexpr double kMinFactor = 0.2;
 constexpr double kMaxFactor = 10.0;
 constexpr double kEtaKeep = 1.5;
+constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
 
 struct Smem {
   double *red;  // 2*32 reduction slots
@@ -34,6 +35,7 @@ struct Smem {
   double *colk; // n (LT-sized use)
   double *wlu;  // n: error-weight scale the stored inverse was formed with
   double *bs;   // n: scaled right-hand side
+  double *V;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
 };
 
 // Sum over the CTA; every thread gets thread 0's total (deterministic).
@@ -308,10 +310,122 @@ __device__ void apply_inverse(const Smem &s, int n, int lda, const double *b, do
   __syncthreads();
 }
 
+// Left-preconditioned GMRES for (I - cJ) x = b, the Newton system of the
+// FP32 path, in the error-weighted coordinates (scale = atol + rtol |y|):
+// the operator is applied in FP64 from the stored sparse Jacobian and the
+// FP32 inverse is only the preconditioner, so the Newton corrections keep
+// FP64 accuracy whatever the single-precision factor loses.  The method is
+// SPGMR's (modified Gram-Schmidt, no restarts, x0 = 0, converged when the
+// preconditioned residual's weighted 2-norm is <= delta), restated from Saad
+// and Schultz, SIAM J. Sci. Stat. Comput. 7 (1986) 856-869; the reference
+// plugin drives it through CVODE with PREC_LEFT / MODIFIED_GS
+// (applications/cfd_plugin/solver_cvode.cpp:119-141, 201-212).  Every thread
+// keeps the same Hessenberg matrix and rotations (the reductions broadcast
+// one total), so no thread-0 phase is needed.  Returns 0 when converged, 1
+// when the residual was reduced but not below delta, 2 otherwise.
+template <class LT>
+__device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda,
+                         double delta, const double *b, double *x) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *V = s.V, *u = s.V + (kMaxl + 1) * n, *z = u + n;
+  apply_inverse<LT>(s, n, lda, b, z);
+  double a = 0.0;
+  for (int i = tid; i < n; i += nt) {
+    const double t = z[i] / s.scale[i];
+    V[i] = t;
+    a += t * t;
+  }
+  const double beta = sqrt(block_sum(a, s.red));
+  if (!isfinite(beta)) return 2;
+  if (beta <= delta) {  // the zero initial guess already satisfies the test
+    for (int i = tid; i < n; i += nt) x[i] = 0.0;
+    __syncthreads();
+    return 0;
+  }
+  double H[kMaxl + 1][kMaxl], cs[kMaxl], sn[kMaxl], g[kMaxl + 1], yk[kMaxl];
+  g[0] = beta;
+  for (int i = tid; i < n; i += nt) V[i] /= beta;
+  int nl = 0;
+  double rho = beta;
+  bool conv = false;
+  for (int l = 0; l < kMaxl; ++l) {
+    const double *vl = V + l * n;
+    double *w = V + (l + 1) * n;
+    for (int i = tid; i < n; i += nt) u[i] = vl[i] * s.scale[i];
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) {  // (I - cJ) u, row i
+      double jx = 0.0;
+      for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) jx += J[m.jr_kk[q]] * u[m.jr_col[q]];
+      s.colk[i] = u[i] - c * jx;
+    }
+    __syncthreads();
+    apply_inverse<LT>(s, n, lda, s.colk, z);
+    for (int i = tid; i < n; i += nt) w[i] = z[i] / s.scale[i];
+    for (int k = 0; k <= l; ++k) {  // modified Gram-Schmidt
+      const double *vk = V + k * n;
+      double d = 0.0;
+      for (int i = tid; i < n; i += nt) d += w[i] * vk[i];
+      const double h = block_sum(d, s.red);
+      H[k][l] = h;
+      for (int i = tid; i < n; i += nt) w[i] -= h * vk[i];
+    }
+    double d2 = 0.0;
+    for (int i = tid; i < n; i += nt) d2 += w[i] * w[i];
+    const double hn = sqrt(block_sum(d2, s.red));
+    for (int k = 0; k < l; ++k) {  // earlier rotations on the new column
+      const double h0 = H[k][l], h1 = H[k + 1][l];
+      H[k][l] = cs[k] * h0 + sn[k] * h1;
+      H[k + 1][l] = -sn[k] * h0 + cs[k] * h1;
+    }
+    const double a0 = H[l][l];
+    double cc, ss;
+    if (hn == 0.0) {
+      cc = 1.0;
+      ss = 0.0;
+    } else if (fabs(hn) > fabs(a0)) {
+      const double t = a0 / hn;
+      ss = 1.0 / sqrt(1.0 + t * t);
+      cc = ss * t;
+    } else {
+      const double t = hn / a0;
+      cc = 1.0 / sqrt(1.0 + t * t);
+      ss = cc * t;
+    }
+    H[l][l] = cc * a0 + ss * hn;
+    cs[l] = cc;
+    sn[l] = ss;
+    g[l + 1] = -ss * g[l];
+    g[l] = cc * g[l];
+    rho = fabs(g[l + 1]);
+    nl = l + 1;
+    if (hn > 0.0)
+      for (int i = tid; i < n; i += nt) w[i] /= hn;
+    if (!isfinite(rho)) return 2;
+    if (rho <= delta) {
+      conv = true;
+      break;
+    }
+    if (hn == 0.0) break;
+  }
+  for (int k = nl - 1; k >= 0; --k) {
+    double t = g[k];
+    for (int j = k + 1; j < nl; ++j) t -= H[k][j] * yk[j];
+    yk[k] = t / H[k][k];
+  }
+  for (int i = tid; i < n; i += nt) {
+    double acc = 0.0;
+    for (int k = 0; k < nl; ++k) acc += yk[k] * V[k * n + i];
+    x[i] = acc * s.scale[i];
+  }
+  __syncthreads();
+  if (conv) return 0;
+  return rho < beta ? 1 : 2;
+}
+
 template <class LT>
 __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
                            double *J, double v, double t_end, double rtol, double atol,
-                           ReactorStats &st, int lda) {
+                           ReactorStats &st, int lda, double &t_done) {
   const int n = m.nsp + 1, tid = threadIdx.x, nt = blockDim.x;
   auto vrms = [&](const double *x, const double *sc) {
     double a = 0.0;
@@ -322,6 +436,8 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
     return sqrt(block_sum(a, s.red) / n);
   };
   double t = 0.0;
+  int rc = 0;
+  t_done = 0.0;
   st.nrhs++;
   if (rhs_cta(m, o, s, v, s.y, s.f0, false, nullptr)) return -1;
   for (int i = tid; i < n; i += nt) s.scale[i] = atol + fabs(s.y[i]) * rtol;
@@ -342,7 +458,8 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   double h = fmin(100.0 * h0, h1);
   h = fmin(h, o.max_dt);
   h = fmin(h, t_end);
-  int q = 1, neq = 0;
+  int q = 1, neq = 0, jac_current = 1, nsteps = 0;
+  double c_lu = h / bc.alp[q], crate = 1.0;
   for (int i = tid; i < (kMaxOrder + 3) * n; i += nt) s.D[i] = 0.0;
   __syncthreads();
   for (int i = tid; i < n; i += nt) {
@@ -351,15 +468,11 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   }
   __syncthreads();
   st.njac++;
-  if (jac_cta(m, o, s, v, s.y, s.f0, J)) return -2;
-  int jac_current = 1;
-  double c_lu = h / bc.alp[q];
+  if (jac_cta(m, o, s, v, s.y, s.f0, J)) { rc = -2; goto failed; }
   st.nlu++;
-  if (invert_cta<LT>(m, s, J, c_lu, n, lda)) return -3;
-  double crate = 1.0;
-  int nsteps = 0;
+  if (invert_cta<LT>(m, s, J, c_lu, n, lda)) { rc = -3; goto failed; }
   while (t < t_end) {
-    if (nsteps >= o.max_steps) return -4;
+    if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
     double safety = 0.9, err_norm = 0.0;
     while (!accepted) {
@@ -371,7 +484,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         change_D_cta(s.D, n, q, (t_end - t) / h);
         h = t_end - t;
       }
-      if (!(t + h > t)) return -5;
+      if (!(t + h > t)) { rc = -5; goto failed; }
       const double t_new = t + h;
       for (int i = tid; i < n; i += nt) {
         double a = 0.0, ps = 0.0;
@@ -389,7 +502,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         st.nlu++;
         c_lu = c;
         crate = 1.0;
-        if (invert_cta<LT>(m, s, J, c, n, lda)) return -3;
+        if (invert_cta<LT>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
       }
       const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
       bool conv = false;
@@ -406,24 +519,21 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         st.nnewt++;
         for (int i = tid; i < n; i += nt) s.tmp[i] = c * s.f[i] - s.psi[i] - s.d[i];
         __syncthreads();
-        apply_inverse<LT>(s, n, lda, s.tmp, s.yp);
+        double gs = gscale;
         if constexpr (sizeof(LT) == sizeof(float)) {
-          // one step of iterative refinement with the residual of the FP64
-          // Newton matrix (I - c_lu J) taken row-wise from the sparse J, so
-          // the single-precision inverse only has to be a contraction
-          for (int i = tid; i < n; i += nt) {
-            double jx = 0.0;
-            for (int p = m.jr_ptr[i]; p < m.jr_ptr[i + 1]; ++p) jx += J[m.jr_kk[p]] * s.yp[m.jr_col[p]];
-            s.colk[i] = s.tmp[i] - (s.yp[i] - c_lu * jx);
-          }
-          __syncthreads();
-          apply_inverse<LT>(s, n, lda, s.colk, s.tmp);
-          for (int i = tid; i < n; i += nt) s.yp[i] += s.tmp[i];
-          __syncthreads();
+          // Krylov tolerance eps_lin * nlscoef / error constant (WRMS), as a
+          // weighted 2-norm; a reduced but unconverged residual is accepted
+          // on the first Newton iteration only
+          const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
+          const int lrc = gmres_cta<LT>(m, s, J, c, n, lda, delta, s.tmp, s.yp);
+          if (lrc == 2 || (lrc == 1 && it > 0)) break;
+          gs = 1.0;  // the Krylov solve uses the current c exactly
+        } else {
+          apply_inverse<LT>(s, n, lda, s.tmp, s.yp);
         }
         double a = 0.0;
         for (int i = tid; i < n; i += nt) {
-          const double dy = s.yp[i] * gscale;
+          const double dy = s.yp[i] * gs;
           s.y[i] += dy;
           s.d[i] += dy;
           const double tt = dy / s.scale[i];
@@ -442,14 +552,14 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
       if (!conv) {
         if (!jac_current) {
           st.nrhs++;
-          if (rhs_cta(m, o, s, v, s.ypred, s.f0, false, nullptr)) return -6;
+          if (rhs_cta(m, o, s, v, s.ypred, s.f0, false, nullptr)) { rc = -6; goto failed; }
           st.njac++;
-          if (jac_cta(m, o, s, v, s.ypred, s.f0, J)) return -2;
+          if (jac_cta(m, o, s, v, s.ypred, s.f0, J)) { rc = -2; goto failed; }
           jac_current = 1;
           st.nlu++;
           c_lu = c;
           crate = 1.0;
-          if (invert_cta<LT>(m, s, J, c, n, lda)) return -3;
+          if (invert_cta<LT>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
           continue;
         }
         change_D_cta(s.D, n, q, 0.5);
@@ -464,7 +574,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         a += e * e;
       }
       err_norm = sqrt(block_sum(a, s.red) / n);
-      if (!isfinite(err_norm)) return -7;
+      if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
         const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D_cta(s.D, n, q, fac);
@@ -520,7 +630,13 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   }
   for (int i = tid; i < n; i += nt) s.y[i] = s.D[i];
   __syncthreads();
+  t_done = t;
   return 0;
+failed:  // D[0] holds the last accepted state (step-size changes keep it)
+  for (int i = tid; i < n; i += nt) s.y[i] = s.D[i];
+  __syncthreads();
+  t_done = t;
+  return rc;
 }
 
 // spill bits: 1 = rates of progress in a global slice, 2 = BDF differences
@@ -551,6 +667,11 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
   s.colk = p; p += n;
   s.wlu = p; p += n;
   s.bs = p; p += n;
+  s.V = nullptr;
+  if (sizeof(LT) == sizeof(float)) {
+    s.V = p;
+    p += (kMaxl + 3) * n;
+  }
   s.piv = (int *)p; p += (n + 1) / 2 + 1;
   s.A = p;
   Consts bc;
@@ -576,9 +697,15 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
+    // retries (solver_cvode.cpp:227-246): restart the method from the last
+    // accepted state for the remaining time with adjusted tolerances;
+    // max_steps counts per attempt
+    double t_left = a.dt;
     for (int attempt = 0;; ++attempt) {
-      rc = attempt_cta<LT>(m, o, bc, s, J, v, a.dt, rtol, atol, rs, lda);
+      double t_done = 0.0;
+      rc = attempt_cta<LT>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
+      t_left -= t_done;
       rs.retries++;
       atol *= o.retry_atol_factor;
       rtol *= o.retry_rtol_factor;
@@ -613,6 +740,7 @@ size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill) {
   const int lda = (n % 2 == 1) ? n : n + 1;  // odd row stride: conflict-free column walks
   if (lda_out) *lda_out = lda;
   size_t d = 72 + 3 * (size_t)m.nsp + 12 * (size_t)n + ((n + 1) / 2 + 1);
+  if (fp32) d += (kMaxl + 3) * (size_t)n;
   if (!(spill & 1)) d += m.nstep;
   if (!(spill & 2)) d += (kMaxOrder + 3) * (size_t)n;
   size_t bytes = d * sizeof(double) + (size_t)n * lda * (fp32 ? sizeof(float) : sizeof(double));

@@ -199,6 +199,7 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
   o.atol = D["abs_tol"];
   o.max_dt = D["max_dt"];
   o.nlscoef = D["nonlinear_convergence_coeff"];
+  o.eps_lin = D["eps_lin"];
   o.max_steps = I["max_steps"];
   o.max_retries = I["cvode_num_retries"];
   o.retry_atol = D["cvode_retry_absolute_tolerance_adjustment"];

@@ -166,6 +166,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.atol = o.atol;
   io.max_dt = o.max_dt;
   io.nlscoef = o.nlscoef;
+  io.eps_lin = o.eps_lin;
   io.max_steps = o.max_steps;
   io.max_retries = std::max(1, o.max_retries);
   io.retry_atol_factor = o.retry_atol;

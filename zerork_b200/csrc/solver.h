@@ -22,6 +22,7 @@ namespace zrk {
 
 struct SolveOptions {
   double rtol = 1.0e-8, atol = 1.0e-20, max_dt = 0.05, nlscoef = 0.05;
+  double eps_lin = 1.0e-3;  // Krylov tolerance factor (FP32 path)
   int max_steps = 5000, max_retries = 5;
   double retry_atol = 0.1, retry_rtol = 1.0;
   double Tref = 1.0, mmf = 1.0e-30, lim = 1.0e22;
