@@ -36,7 +36,8 @@ def _flags(src):
 
 def _compile(src, verbose=False):
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
-    headers = glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+               glob.glob(os.path.join(HERE, "..", "include", "*.h")))
     newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in headers])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj, ""

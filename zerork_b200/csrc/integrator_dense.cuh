@@ -1,0 +1,855 @@
+// integrator_dense.cuh -- CTA-per-reactor BDF integration with the Newton
+// matrix held as one dense block in shared memory.
+//
+// The symbolic factorization of the reactor Newton matrix P = I - cJ
+// (sparse_lu.h) fills 64-100 % of the dense n x n block for the benchmark
+// mechanisms, so the factor is handled as a single dense supernode: P is
+// inverted in shared memory by Gauss-Jordan elimination with partial
+// pivoting, and every Newton solve is a parallel matrix-vector product.  A
+// persistent CTA takes reactors from the work queue; the reactor's BDF state
+// (differences, iterate, right-hand sides, weights) and the rate workspace
+// live in shared memory, the reactor Jacobian in global memory.  Step
+// control is the same as integrator.cu (Shampine-Reichelt BDF with CVODE's
+// Newton test and step hysteresis).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "integrator.h"
+#include "kinetics_dev.cuh"
+
+namespace zrk {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kNewtonMaxIter = 3;
+constexpr double kMinFactor = 0.2;
+constexpr double kMaxFactor = 10.0;
+constexpr double kEtaKeep = 1.5;
+constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
+
+struct Smem {
+  double *red;  // 128 slots: block sums [0, 33), pivot candidates [64, 112)
+  double *C, *G, *U, *ROP;
+  double *D, *y, *f, *f0, *ypred, *psi, *d, *scale, *tmp, *yp;
+  void *A;      // n x lda inverse (LT)
+  int *perm;    // n: row i of the factored matrix is scaled row perm[i]
+  double *colk; // n (LT-sized use)
+  double *wlu;  // n: error-weight scale the stored inverse was formed with
+  double *bs;   // n: scaled right-hand side
+  double *V;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
+};
+
+// Sum over the CTA; every thread gets thread 0's total (deterministic).
+__device__ __forceinline__ double block_sum(double v, double *red) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < nw; ++i) s += red[i];
+    red[32] = s;
+  }
+  __syncthreads();
+  return red[32];
+}
+
+// ydot at y (shared vector); returns 1 if T <= 0 (all threads agree).
+__device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v,
+                       const double *y, double *ydot, bool clamp, double *cv_out) {
+  const int S = m.nsp, tid = threadIdx.x, nt = blockDim.x;
+  const double yS = y[S];
+  double T = yS * o.Tref;
+  if (!(T > 0.0)) return 1;
+  if (T > 1.0e4) T = 1.0e4;
+  const double logT = log(T), invT = 1.0 / T, lprt = log(kPatmD / (kRuD * T));
+  const double dens = 1.0 / v;
+  double pc = 0.0, pcv = 0.0;
+  for (int k = tid; k < S; k += nt) {
+    double ys = y[k];
+    if (clamp) ys = clamp_mass_fraction(ys, o.mmf);
+    const double c = dens * m.inv_mw[k] * ys;
+    s.C[k] = c;
+    double cp, h, g;
+    nasa_cp_h_g(m.thermo + 16 * k, T, logT, &cp, &h, &g);
+    s.G[k] = g;
+    s.U[k] = h - 1.0;
+    pc += c;
+    pcv += ((cp - 1.0) * m.ru_inv_mw[k]) * ys;
+  }
+  const double Csum = block_sum(pc, s.red);
+  const double cv = block_sum(pcv, s.red);
+  for (int r = tid; r < m.nrxn; r += nt)
+    reaction_item<1, 1>(m, m.rxn[r], 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum, o.lim);
+  __syncthreads();
+  double pe = 0.0;
+  for (int k = tid; k < S; k += nt) {
+    double des = 0.0, cre = 0.0;
+    for (int q = m.sd_ptr[k]; q < m.sd_ptr[k + 1]; ++q) des += s.ROP[m.sd_step[q]];
+    for (int q = m.sc_ptr[k]; q < m.sc_ptr[k + 1]; ++q) cre += s.ROP[m.sc_step[q]];
+    const double net = cre - des;
+    ydot[k] = net * m.mw[k] * v;
+    pe += s.U[k] * net * v;
+  }
+  const double es = block_sum(pe, s.red);
+  if (tid == 0) ydot[S] = -es * kRuD * yS / cv + 0.0;
+  if (cv_out) *cv_out = cv;
+  __syncthreads();
+  return 0;
+}
+
+// Reactor Jacobian (SetupJacobianSparse semantics) into J (global, nnz).
+__device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v,
+                       const double *y, const double *fy, double *J) {
+  const int S = m.nsp, tid = threadIdx.x, nt = blockDim.x;
+  int need = 0;
+  for (int k = tid; k < S; k += nt) need |= (fabs(y[k]) < o.mmf);
+  need = __syncthreads_or(need);
+  double cvc;
+  if (rhs_cta(m, o, s, v, y, s.tmp, need != 0, &cvc)) return 1;
+  const double TdC = s.tmp[S];
+  const double yS = y[S];
+  const double RuTemp = kRuD * yS;
+  const double multFact = -1.0 / cvc;
+  double T = yS * o.Tref;
+  if (T > 1.0e4) T = 1.0e4;
+  for (int j = tid; j < S; j += nt) {  // one column per thread
+    const double t2 = m.mw[j] / clamp_mass_fraction(y[j], o.mmf) * v;
+    const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
+    const double wcol = m.inv_mw[j];
+    double trow = 0.0;
+    for (int kk = k0; kk < k1; ++kk) {
+      const int row = m.row_idx[kk];
+      double des = 0.0, cre = 0.0;
+      for (int q = m.nzd_ptr[kk]; q < m.nzd_ptr[kk + 1]; ++q) des += s.ROP[m.nzd_step[q]];
+      for (int q = m.nzc_ptr[kk]; q < m.nzc_ptr[kk + 1]; ++q) cre += s.ROP[m.nzc_step[q]];
+      const double val = (0.0 - des * t2) + cre * t2;
+      trow += val * s.U[row];
+      J[kk] = val * (m.mw[row] * wcol);
+    }
+    const double cvj = (nasa_cp(m.thermo + 16 * j, T) - 1.0) * m.ru_inv_mw[j];
+    double tr = trow * RuTemp;
+    tr += TdC * cvj * m.mw[j];
+    tr *= wcol * multFact;
+    J[k1] = tr;
+  }
+  __syncthreads();
+  const double ySp = yS + yS * o.sqrt_ur;
+  const double mult = 1.0 / (ySp - yS);
+  for (int k = tid; k < S; k += nt) s.yp[k] = y[k];
+  if (tid == 0) s.yp[S] = ySp;
+  __syncthreads();
+  if (rhs_cta(m, o, s, v, s.yp, s.tmp, false, nullptr)) return 1;
+  for (int kk = m.col_ptr[S] + tid; kk < m.col_ptr[S + 1]; kk += nt) {
+    const int row = m.row_idx[kk];
+    J[kk] = (s.tmp[row] - fy[row]) * mult;
+  }
+  __syncthreads();
+  return 0;
+}
+
+// Newton matrix inverse in shared memory, formed in error-weight-scaled
+// coordinates: Pw = W^-1 (I - cJ) W with W = diag(scale), scale = atol +
+// rtol |y| of the current step, so entry (i, j) is P_ij scale_j / scale_i,
+// the Jacobian of relative changes.  It is far better balanced than P for
+// species spanning 20 decades of mass fraction and keeps the inverse
+// accurate in the weighted norm the Newton test uses.
+//
+// Gauss-Jordan with partial pivoting, in place.  Row interchanges are
+// accumulated in perm (row i of the factored matrix is row perm[i] of Pw),
+// so A ends as (Pi Pw)^-1 = Pw^-1 Pi^T and the right-hand side is permuted on
+// application instead of unswapping columns.  Two barriers per pivot: phase
+// S picks the pivot from the per-warp candidates (every thread computes the
+// same choice), swaps the rows and scales the pivot row; phase U updates the
+// other rows, warp w owning rows i = w (mod warps), two rows per pass with
+// every load issued before the stores, lane l the columns l (mod 32) with
+// the pivot row in registers, and leaves the candidate for the next column.
+// Returns nonzero (all threads) for a singular or non-finite matrix.
+template <class LT>
+__device__ __forceinline__ void track(double &ca, int &ci, double &cv, LT a, int i) {
+  const double d = fabs((double)a);
+  if (d > ca) {
+    ca = d;
+    ci = i;
+    cv = (double)a;
+  }
+}
+
+// Largest |value| over the warp, ties to the lowest row; every lane ends
+// with the same (a, i, v).
+__device__ __forceinline__ void warp_argmax(double &a, int &i, double &v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double oa = __shfl_xor_sync(kFull, a, o), ov = __shfl_xor_sync(kFull, v, o);
+    const int oi = __shfl_xor_sync(kFull, i, o);
+    if (oa > a || (oa == a && oi < i)) {
+      a = oa;
+      i = oi;
+      v = ov;
+    }
+  }
+}
+
+template <class LT, int NC>
+__device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda) {
+  LT *A = (LT *)s.A;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
+  double *cand = s.red + 64;  // [0, 16): |pivot|, [16, 32): row, [32, 48): value
+  for (int i = tid; i < n * lda; i += nt) A[i] = (LT)0;
+  for (int i = tid; i < n; i += nt) {
+    s.wlu[i] = s.scale[i];
+    s.perm[i] = i;
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += nt) {  // Jacobian row i from the row-wise view
+    const double ci = -c / s.wlu[i];
+    for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) {
+      const int j = m.jr_col[q];
+      A[i * lda + j] = (LT)(ci * J[m.jr_kk[q]] * s.wlu[j]);
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < n; i += nt) A[i * lda + i] += (LT)1;
+  __syncthreads();
+  {  // candidates for column 0
+    double ca = -1.0, cv = 0.0;
+    int ci = n;
+    for (int i = tid; i < n; i += nt) track(ca, ci, cv, A[i * lda], i);
+    warp_argmax(ca, ci, cv);
+    if (lane == 0) {
+      cand[w] = ca;
+      cand[16 + w] = (double)ci;
+      cand[32 + w] = cv;
+    }
+  }
+  __syncthreads();
+  int bad = 0;
+  for (int k = 0; k < n; ++k) {
+    // ---- phase S: pivot (warp argmax over the warp candidates, the same in
+    // every warp), row interchange, scaled pivot row
+    double best = lane < nw ? cand[lane] : -1.0, pv = lane < nw ? cand[32 + lane] : 0.0;
+    int p = lane < nw ? (int)cand[16 + lane] : n;
+    warp_argmax(best, p, pv);
+    if (!(best > 0.0) || !isfinite(best) || p >= n) {
+      bad = 1;
+      break;  // uniform: every thread made the same choice
+    }
+    const LT pinv = (LT)1 / (LT)pv;
+    if (tid == 0) {
+      const int t = s.perm[k];
+      s.perm[k] = s.perm[p];
+      s.perm[p] = t;
+    }
+    for (int j = tid; j < n; j += nt) {
+      const LT a = A[k * lda + j], b = A[p * lda + j];
+      A[p * lda + j] = a;
+      A[k * lda + j] = (j == k ? (LT)1 : b) * pinv;
+    }
+    __syncthreads();
+    // ---- phase U: eliminate column k from every other row.  The register
+    // copy of the pivot row holds 0 in column k, so the uniform update
+    // leaves that entry as it is, and the lane owning column k then stores
+    // its Gauss-Jordan value -f pinv (program order: no race).
+    LT akv[NC];
+    const int ck = k & 31;
+#pragma unroll
+    for (int t = 0; t < NC; ++t) {
+      const int j = lane + 32 * t;
+      akv[t] = (t < NC - 1 || j < n) ? A[k * lda + j] : (LT)0;
+      if (t == (k >> 5) && lane == ck) akv[t] = (LT)0;
+    }
+    const int t1 = (k + 1) >> 5, c1 = (k + 1) & 31;
+    double ca = -1.0, cv = 0.0;
+    int ci = n;
+    for (int i0 = w; i0 < n; i0 += 2 * nw) {
+      const int i1 = i0 + nw;
+      const bool in1 = i1 < n;
+      const LT f0 = (i0 != k) ? A[i0 * lda + k] : (LT)0;  // broadcast reads
+      const LT f1 = (in1 && i1 != k) ? A[i1 * lda + k] : (LT)0;
+      LT a0[NC], a1[NC];
+#pragma unroll
+      for (int t = 0; t < NC; ++t) {
+        const int j = lane + 32 * t;
+        const bool jv = t < NC - 1 || j < n;
+        a0[t] = jv ? A[i0 * lda + j] : (LT)0;
+        a1[t] = (jv && in1) ? A[i1 * lda + j] : (LT)0;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < NC; ++t) {
+        const int j = lane + 32 * t;
+        const bool jv = t < NC - 1 || j < n;
+        a0[t] -= f0 * akv[t];
+        a1[t] -= f1 * akv[t];
+        if (jv && f0 != (LT)0) A[i0 * lda + j] = a0[t];
+        if (jv && f1 != (LT)0) A[i1 * lda + j] = a1[t];
+      }
+      if (lane == ck) {
+        if (f0 != (LT)0) A[i0 * lda + k] = -f0 * pinv;
+        if (f1 != (LT)0) A[i1 * lda + k] = -f1 * pinv;
+      }
+      if (lane == c1 && k + 1 < n) {  // candidates for column k + 1
+        LT v0 = a0[0], v1 = a1[0];
+#pragma unroll
+        for (int t = 1; t < NC; ++t)
+          if (t == t1) {
+            v0 = a0[t];
+            v1 = a1[t];
+          }
+        if (i0 > k) track(ca, ci, cv, v0, i0);
+        if (in1 && i1 > k) track(ca, ci, cv, v1, i1);
+      }
+    }
+    warp_argmax(ca, ci, cv);
+    if (lane == 0) {
+      cand[w] = ca;
+      cand[16 + w] = (double)ci;
+      cand[32 + w] = cv;
+    }
+    __syncthreads();
+  }
+  return __syncthreads_or(bad);
+}
+
+// x = (I - c_lu J)^{-1} b with the stored inverse: x = W A (perm of W^-1 b).
+// Thread per row, four independent partial sums to hide the FMA latency.
+template <class LT>
+__device__ void apply_inverse(const Smem &s, int n, int lda, const double *b, double *x) {
+  const LT *A = (const LT *)s.A;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int pi = s.perm[i];
+    s.bs[i] = b[pi] / s.wlu[pi];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const LT *row = A + (size_t)i * lda;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int j = 0;
+    for (; j + 3 < n; j += 4) {
+      a0 += (double)row[j] * s.bs[j];
+      a1 += (double)row[j + 1] * s.bs[j + 1];
+      a2 += (double)row[j + 2] * s.bs[j + 2];
+      a3 += (double)row[j + 3] * s.bs[j + 3];
+    }
+    for (; j < n; ++j) a0 += (double)row[j] * s.bs[j];
+    x[i] = ((a0 + a1) + (a2 + a3)) * s.wlu[i];
+  }
+  __syncthreads();
+}
+
+
+__device__ void change_D_cta(double *D, int n, int order, double fac) {
+  double R[kMaxOrder + 1][kMaxOrder + 1], U[kMaxOrder + 1][kMaxOrder + 1];
+  for (int pass = 0; pass < 2; ++pass) {
+    const double f = pass == 0 ? fac : 1.0;
+    double (*A)[kMaxOrder + 1] = pass == 0 ? R : U;
+    for (int j = 0; j <= order; ++j) {
+      A[0][j] = 1.0;
+      for (int i = 1; i <= order; ++i) A[i][j] = A[i - 1][j] * (j == 0 ? 0.0 : (i - 1 - f * j) / i);
+    }
+  }
+  double RU[kMaxOrder + 1][kMaxOrder + 1];
+  for (int i = 0; i <= order; ++i)
+    for (int j = 0; j <= order; ++j) {
+      double t = 0.0;
+      for (int k = 0; k <= order; ++k) t += R[i][k] * U[k][j];
+      RU[i][j] = t;
+    }
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    double old[kMaxOrder + 1];
+    for (int k = 0; k <= order; ++k) old[k] = D[k * n + c];
+    for (int i = 0; i <= order; ++i) {
+      double t = 0.0;
+      for (int k = 0; k <= order; ++k) t += RU[k][i] * old[k];
+      D[i * n + c] = t;
+    }
+  }
+  __syncthreads();
+}
+
+struct Consts {
+  double gam[kMaxOrder + 2], alp[kMaxOrder + 2], econ[kMaxOrder + 2];
+};
+
+__device__ void make_consts(Consts &b) {
+  const double kap[kMaxOrder + 1] = {0.0, -0.1850, -1.0 / 9.0, -0.0823, -0.0415, 0.0};
+  for (int k = 0; k <= kMaxOrder + 1; ++k) {
+    double g = 0.0;
+    for (int i = 1; i <= k; ++i) g += 1.0 / i;
+    b.gam[k] = g;
+    const double kk = (k <= kMaxOrder) ? kap[k] : 0.0;
+    b.alp[k] = (1.0 - kk) * g;
+    b.econ[k] = kk * g + 1.0 / (k + 1);
+  }
+}
+
+
+// Left-preconditioned GMRES for (I - cJ) x = b, the Newton system of the
+// FP32 path, in the error-weighted coordinates (scale = atol + rtol |y|):
+// the operator is applied in FP64 from the stored sparse Jacobian and the
+// FP32 inverse is only the preconditioner, so the Newton corrections keep
+// FP64 accuracy whatever the single-precision factor loses.  The method is
+// SPGMR's (modified Gram-Schmidt, no restarts, x0 = 0, converged when the
+// preconditioned residual's weighted 2-norm is <= delta), restated from Saad
+// and Schultz, SIAM J. Sci. Stat. Comput. 7 (1986) 856-869; the reference
+// plugin drives it through CVODE with PREC_LEFT / MODIFIED_GS
+// (applications/cfd_plugin/solver_cvode.cpp:119-141, 201-212).  Every thread
+// keeps the same Hessenberg matrix and rotations (the reductions broadcast
+// one total), so no thread-0 phase is needed.  Returns 0 when converged, 1
+// when the residual was reduced but not below delta, 2 otherwise.
+template <class LT>
+__device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda,
+                         double delta, const double *b, double *x) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  double *V = s.V, *u = s.V + (kMaxl + 1) * n, *z = u + n;
+  apply_inverse<LT>(s, n, lda, b, z);
+  double a = 0.0;
+  for (int i = tid; i < n; i += nt) {
+    const double t = z[i] / s.scale[i];
+    V[i] = t;
+    a += t * t;
+  }
+  const double beta = sqrt(block_sum(a, s.red));
+  if (!isfinite(beta)) return 2;
+  if (beta <= delta) {  // the zero initial guess already satisfies the test
+    for (int i = tid; i < n; i += nt) x[i] = 0.0;
+    __syncthreads();
+    return 0;
+  }
+  double H[kMaxl + 1][kMaxl], cs[kMaxl], sn[kMaxl], g[kMaxl + 1], yk[kMaxl];
+  g[0] = beta;
+  for (int i = tid; i < n; i += nt) V[i] /= beta;
+  int nl = 0;
+  double rho = beta;
+  bool conv = false;
+  for (int l = 0; l < kMaxl; ++l) {
+    const double *vl = V + l * n;
+    double *w = V + (l + 1) * n;
+    for (int i = tid; i < n; i += nt) u[i] = vl[i] * s.scale[i];
+    __syncthreads();
+    for (int i = tid; i < n; i += nt) {  // (I - cJ) u, row i
+      double jx = 0.0;
+      for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) jx += J[m.jr_kk[q]] * u[m.jr_col[q]];
+      s.colk[i] = u[i] - c * jx;
+    }
+    __syncthreads();
+    apply_inverse<LT>(s, n, lda, s.colk, z);
+    for (int i = tid; i < n; i += nt) w[i] = z[i] / s.scale[i];
+    for (int k = 0; k <= l; ++k) {  // modified Gram-Schmidt
+      const double *vk = V + k * n;
+      double d = 0.0;
+      for (int i = tid; i < n; i += nt) d += w[i] * vk[i];
+      const double h = block_sum(d, s.red);
+      H[k][l] = h;
+      for (int i = tid; i < n; i += nt) w[i] -= h * vk[i];
+    }
+    double d2 = 0.0;
+    for (int i = tid; i < n; i += nt) d2 += w[i] * w[i];
+    const double hn = sqrt(block_sum(d2, s.red));
+    for (int k = 0; k < l; ++k) {  // earlier rotations on the new column
+      const double h0 = H[k][l], h1 = H[k + 1][l];
+      H[k][l] = cs[k] * h0 + sn[k] * h1;
+      H[k + 1][l] = -sn[k] * h0 + cs[k] * h1;
+    }
+    const double a0 = H[l][l];
+    double cc, ss;
+    if (hn == 0.0) {
+      cc = 1.0;
+      ss = 0.0;
+    } else if (fabs(hn) > fabs(a0)) {
+      const double t = a0 / hn;
+      ss = 1.0 / sqrt(1.0 + t * t);
+      cc = ss * t;
+    } else {
+      const double t = hn / a0;
+      cc = 1.0 / sqrt(1.0 + t * t);
+      ss = cc * t;
+    }
+    H[l][l] = cc * a0 + ss * hn;
+    cs[l] = cc;
+    sn[l] = ss;
+    g[l + 1] = -ss * g[l];
+    g[l] = cc * g[l];
+    rho = fabs(g[l + 1]);
+    nl = l + 1;
+    if (hn > 0.0)
+      for (int i = tid; i < n; i += nt) w[i] /= hn;
+    if (!isfinite(rho)) return 2;
+    if (rho <= delta) {
+      conv = true;
+      break;
+    }
+    if (hn == 0.0) break;
+  }
+  for (int k = nl - 1; k >= 0; --k) {
+    double t = g[k];
+    for (int j = k + 1; j < nl; ++j) t -= H[k][j] * yk[j];
+    yk[k] = t / H[k][k];
+  }
+  for (int i = tid; i < n; i += nt) {
+    double acc = 0.0;
+    for (int k = 0; k < nl; ++k) acc += yk[k] * V[k * n + i];
+    x[i] = acc * s.scale[i];
+  }
+  __syncthreads();
+  if (conv) return 0;
+  return rho < beta ? 1 : 2;
+}
+
+template <class LT, int NC>
+__device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
+                           double *J, double v, double t_end, double rtol, double atol,
+                           ReactorStats &st, int lda, double &t_done) {
+  const int n = m.nsp + 1, tid = threadIdx.x, nt = blockDim.x;
+  auto vrms = [&](const double *x, const double *sc) {
+    double a = 0.0;
+    for (int i = tid; i < n; i += nt) {
+      const double t = x[i] / sc[i];
+      a += t * t;
+    }
+    return sqrt(block_sum(a, s.red) / n);
+  };
+  double t = 0.0;
+  int rc = 0;
+  t_done = 0.0;
+  st.nrhs++;
+  if (rhs_cta(m, o, s, v, s.y, s.f0, false, nullptr)) return -1;
+  for (int i = tid; i < n; i += nt) s.scale[i] = atol + fabs(s.y[i]) * rtol;
+  __syncthreads();
+  const double d0 = vrms(s.y, s.scale), d1 = vrms(s.f0, s.scale);
+  double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
+  if (h0 > t_end) h0 = t_end;
+  for (int i = tid; i < n; i += nt) s.tmp[i] = s.y[i] + h0 * s.f0[i];
+  __syncthreads();
+  double d2 = 0.0;
+  st.nrhs++;
+  if (rhs_cta(m, o, s, v, s.tmp, s.f, false, nullptr) == 0) {
+    for (int i = tid; i < n; i += nt) s.d[i] = s.f[i] - s.f0[i];
+    __syncthreads();
+    d2 = vrms(s.d, s.scale) / h0;
+  }
+  double h1 = (d1 <= 1e-15 && d2 <= 1e-15) ? fmax(1e-6, h0 * 1e-3) : sqrt(0.01 / fmax(d1, d2));
+  double h = fmin(100.0 * h0, h1);
+  h = fmin(h, o.max_dt);
+  h = fmin(h, t_end);
+  int q = 1, neq = 0, jac_current = 1, nsteps = 0;
+  double c_lu = h / bc.alp[q], crate = 1.0;
+  for (int i = tid; i < (kMaxOrder + 3) * n; i += nt) s.D[i] = 0.0;
+  __syncthreads();
+  for (int i = tid; i < n; i += nt) {
+    s.D[i] = s.y[i];
+    s.D[n + i] = s.f0[i] * h;
+  }
+  __syncthreads();
+  st.njac++;
+  if (jac_cta(m, o, s, v, s.y, s.f0, J)) { rc = -2; goto failed; }
+  st.nlu++;
+  if (invert_cta<LT, NC>(m, s, J, c_lu, n, lda)) { rc = -3; goto failed; }
+  while (t < t_end) {
+    if (nsteps >= o.max_steps) { rc = -4; goto failed; }
+    bool accepted = false;
+    double safety = 0.9, err_norm = 0.0;
+    while (!accepted) {
+      if (h > o.max_dt) {
+        change_D_cta(s.D, n, q, o.max_dt / h);
+        h = o.max_dt;
+      }
+      if (t + h > t_end) {
+        change_D_cta(s.D, n, q, (t_end - t) / h);
+        h = t_end - t;
+      }
+      if (!(t + h > t)) { rc = -5; goto failed; }
+      const double t_new = t + h;
+      for (int i = tid; i < n; i += nt) {
+        double a = 0.0, ps = 0.0;
+        for (int k = 0; k <= q; ++k) a += s.D[k * n + i];
+        for (int k = 1; k <= q; ++k) ps += bc.gam[k] * s.D[k * n + i];
+        s.ypred[i] = a;
+        s.psi[i] = ps / bc.alp[q];
+        s.scale[i] = atol + rtol * fabs(a);
+        s.y[i] = a;
+        s.d[i] = 0.0;
+      }
+      __syncthreads();
+      const double c = h / bc.alp[q];
+      if (fabs(c / c_lu - 1.0) > 0.3) {
+        st.nlu++;
+        c_lu = c;
+        crate = 1.0;
+        if (invert_cta<LT, NC>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
+      }
+      const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
+      bool conv = false;
+      int it;
+      double dnorm_old = -1.0;
+      for (it = 0; it < kNewtonMaxIter; ++it) {
+        st.nrhs++;
+        if (rhs_cta(m, o, s, v, s.y, s.f, false, nullptr)) break;
+        int bad = 0;
+        for (int i = tid; i < n; i += nt) bad |= !isfinite(s.f[i]);
+        if (__syncthreads_or(bad)) break;
+        if (it == 0)
+          for (int i = tid; i < n; i += nt) s.f0[i] = s.f[i];
+        st.nnewt++;
+        for (int i = tid; i < n; i += nt) s.tmp[i] = c * s.f[i] - s.psi[i] - s.d[i];
+        __syncthreads();
+        double gs = gscale;
+        if constexpr (sizeof(LT) == sizeof(float)) {
+          // Krylov tolerance eps_lin * nlscoef / error constant (WRMS), as a
+          // weighted 2-norm.  Unlike CVODE, which accepts a reduced but
+          // unconverged residual on the first Newton iteration, every solve
+          // must converge: with a single-precision preconditioner a stalled
+          // Krylov solve can pass the Newton test with a poor correction,
+          // and a failure here costs only a Jacobian update or a step cut.
+          const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
+          if (gmres_cta<LT>(m, s, J, c, n, lda, delta, s.tmp, s.yp) != 0) break;
+          gs = 1.0;  // the Krylov solve uses the current c exactly
+        } else {
+          apply_inverse<LT>(s, n, lda, s.tmp, s.yp);
+        }
+        double a = 0.0;
+        for (int i = tid; i < n; i += nt) {
+          const double dy = s.yp[i] * gs;
+          s.y[i] += dy;
+          s.d[i] += dy;
+          const double tt = dy / s.scale[i];
+          a += tt * tt;
+        }
+        const double dn = sqrt(block_sum(a, s.red) / n);
+        if (dnorm_old > 0.0) crate = fmax(0.3 * crate, dn / dnorm_old);
+        if (bc.econ[q] * dn * fmin(1.0, crate) <= o.nlscoef) {
+          conv = true;
+          ++it;
+          break;
+        }
+        if (dnorm_old > 0.0 && dn > 2.0 * dnorm_old) break;
+        dnorm_old = dn;
+      }
+      if (!conv) {
+        if (!jac_current) {
+          st.nrhs++;
+          if (rhs_cta(m, o, s, v, s.ypred, s.f0, false, nullptr)) { rc = -6; goto failed; }
+          st.njac++;
+          if (jac_cta(m, o, s, v, s.ypred, s.f0, J)) { rc = -2; goto failed; }
+          jac_current = 1;
+          st.nlu++;
+          c_lu = c;
+          crate = 1.0;
+          if (invert_cta<LT, NC>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
+          continue;
+        }
+        change_D_cta(s.D, n, q, 0.5);
+        h *= 0.5;
+        st.nrej++;
+        continue;
+      }
+      safety = 0.9 * (2 * kNewtonMaxIter + 1) / (2.0 * kNewtonMaxIter + it);
+      double a = 0.0;
+      for (int i = tid; i < n; i += nt) {
+        const double e = bc.econ[q] * s.d[i] / s.scale[i];
+        a += e * e;
+      }
+      err_norm = sqrt(block_sum(a, s.red) / n);
+      if (!isfinite(err_norm)) { rc = -7; goto failed; }
+      if (err_norm > 1.0) {
+        const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
+        change_D_cta(s.D, n, q, fac);
+        h *= fac;
+        st.nrej++;
+        continue;
+      }
+      accepted = true;
+      t = t_new;
+    }
+    ++nsteps;
+    st.nsteps++;
+    ++neq;
+    jac_current = 0;
+    for (int i = tid; i < n; i += nt) {
+      const double di = s.d[i];
+      s.D[(q + 2) * n + i] = di - s.D[(q + 1) * n + i];
+      s.D[(q + 1) * n + i] = di;
+      for (int k = q; k >= 0; --k) s.D[k * n + i] += s.D[(k + 1) * n + i];
+    }
+    __syncthreads();
+    if (neq < q + 1) continue;
+    double em = INFINITY, ep = INFINITY;
+    {
+      double am = 0.0, ap = 0.0;
+      for (int i = tid; i < n; i += nt) {
+        if (q > 1) {
+          const double e = bc.econ[q - 1] * s.D[q * n + i] / s.scale[i];
+          am += e * e;
+        }
+        if (q < kMaxOrder) {
+          const double e = bc.econ[q + 1] * s.D[(q + 2) * n + i] / s.scale[i];
+          ap += e * e;
+        }
+      }
+      const double sm = block_sum(am, s.red), sp = block_sum(ap, s.red);
+      if (q > 1) em = sqrt(sm / n);
+      if (q < kMaxOrder) ep = sqrt(sp / n);
+    }
+    const double fm = (q > 1) ? pow(em, -1.0 / q) : 0.0;
+    const double f0 = pow(err_norm, -1.0 / (q + 1));
+    const double fp = (q < kMaxOrder) ? pow(ep, -1.0 / (q + 2)) : 0.0;
+    int dq = 0;
+    double best = f0;
+    if (fm > best) { best = fm; dq = -1; }
+    if (fp > best) { best = fp; dq = 1; }
+    q += dq;
+    double fac = fmin(kMaxFactor, safety * best);
+    if (fac < kEtaKeep) fac = 1.0;
+    change_D_cta(s.D, n, q, fac);
+    h *= fac;
+    neq = 0;
+  }
+  for (int i = tid; i < n; i += nt) s.y[i] = s.D[i];
+  __syncthreads();
+  t_done = t;
+  return 0;
+failed:  // D[0] holds the last accepted state (step-size changes keep it)
+  for (int i = tid; i < n; i += nt) s.y[i] = s.D[i];
+  __syncthreads();
+  t_done = t;
+  return rc;
+}
+
+// spill bits: 1 = rates of progress in a global slice, 2 = BDF differences
+// in a global slice (both L2-resident: one slice per resident CTA).
+template <class LT, int NC>
+__global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, IntegOpts o, IntegArgs a,
+                                                                 int lda, int spill) {
+  extern __shared__ double smem_dyn[];
+  const int S = m.nsp, n = S + 1, N = m.nstep, tid = threadIdx.x, nt = blockDim.x;
+  Smem s;
+  double *p = smem_dyn;
+  double *g = a.rop_scratch + (size_t)blockIdx.x * ((size_t)N + (kMaxOrder + 3) * (size_t)n);
+  s.red = p; p += 128;
+  s.C = p; p += S;
+  s.G = p; p += S;
+  s.U = p; p += S;
+  if (spill & 1) { s.ROP = g; } else { s.ROP = p; p += N; }
+  if (spill & 2) { s.D = g + N; } else { s.D = p; p += (kMaxOrder + 3) * n; }
+  s.y = p; p += n;
+  s.f = p; p += n;
+  s.f0 = p; p += n;
+  s.ypred = p; p += n;
+  s.psi = p; p += n;
+  s.d = p; p += n;
+  s.scale = p; p += n;
+  s.tmp = p; p += n;
+  s.yp = p; p += n;
+  s.colk = p; p += n;
+  s.wlu = p; p += n;
+  s.bs = p; p += n;
+  s.V = nullptr;
+  if (sizeof(LT) == sizeof(float)) {
+    s.V = p;
+    p += (kMaxl + 3) * n;
+  }
+  s.perm = (int *)p; p += (n + 1) / 2 + 1;
+  s.A = p;
+  Consts bc;
+  make_consts(bc);
+  __shared__ int next;
+  for (;;) {
+    if (tid == 0) next = atomicAdd(a.queue_head, 1);
+    __syncthreads();
+    const int idx = next;
+    __syncthreads();
+    if (idx >= a.n_reactors) break;
+    const int r = a.order ? a.order[idx] : idx;
+    double *J = a.state + (size_t)r * a.state_stride;
+    const double T0 = a.T[r], P0 = a.P[r];
+    const double *Y0 = a.Y + (size_t)r * S;
+    double pa = 0.0;
+    for (int k = tid; k < S; k += nt) pa += Y0[k] * m.inv_mw[k];
+    const double mwmix = 1.0 / block_sum(pa, s.red);
+    const double v = 1.0 / (P0 * mwmix / (kRuD * T0));
+    for (int k = tid; k < S; k += nt) s.y[k] = Y0[k];
+    if (tid == 0) s.y[S] = T0 / o.Tref;
+    __syncthreads();
+    ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
+    double rtol = o.rtol, atol = o.atol;
+    int rc = 0;
+    // retries (solver_cvode.cpp:227-246): restart the method from the last
+    // accepted state for the remaining time with adjusted tolerances;
+    // max_steps counts per attempt
+    double t_left = a.dt;
+    for (int attempt = 0;; ++attempt) {
+      double t_done = 0.0;
+      rc = attempt_cta<LT, NC>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done);
+      if (rc == 0 || attempt + 1 >= o.max_retries) break;
+      t_left -= t_done;
+      rs.retries++;
+      atol *= o.retry_atol_factor;
+      rtol *= o.retry_rtol_factor;
+    }
+    rs.status = rc;
+    if (rc == 0) {
+      double pb = 0.0;
+      for (int k = tid; k < S; k += nt) {
+        const double ys = s.y[k];
+        a.Y[(size_t)r * S + k] = ys;
+        pb += ys * m.inv_mw[k];
+      }
+      const double mw2 = 1.0 / block_sum(pb, s.red);
+      if (tid == 0) {
+        const double Tn = s.y[S] * o.Tref;
+        a.T[r] = Tn;
+        a.P[r] = kRuD * Tn / (v * mw2);
+      }
+    }
+    if (tid == 0) {
+      a.v[r] = v;
+      if (a.stats) a.stats[r] = rs;
+    }
+    __syncthreads();
+  }
+}
+
+
+template <class LT, int NC>
+cudaError_t launch_dense(const DevMech &m, const IntegOpts &o, const IntegArgs &a, int threads,
+                         int ctas, int spill, size_t smem, int lda, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(integrate_dense_kernel<LT, NC>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  integrate_dense_kernel<LT, NC><<<ctas, threads, smem, stream>>>(m, o, a, lda, spill);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+// Launch for one register-chunk count NC = ceil((nsp + 1) / 32); one
+// translation unit per NC (integrator_dense_ncN.cu) so they compile in parallel.
+cudaError_t launch_integrate_dense_nc1(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc2(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc3(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc4(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc5(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc6(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc7(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+cudaError_t launch_integrate_dense_nc8(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                        int threads, int ctas, int spill, size_t smem, int lda,
+                                        cudaStream_t stream);
+
+}  // namespace zrk

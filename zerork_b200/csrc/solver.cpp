@@ -110,7 +110,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   // BDF differences to an L2-resident global slice if needed
   int spill = -1;
   for (int sp : {0, 1, 3})
-    if (dense_smem_bytes(m, o.lu_fp32, nullptr, sp) <= kSmemMax) {
+    if (m.nsp + 1 <= kDenseMaxN && dense_smem_bytes(m, o.lu_fp32, nullptr, sp) <= kSmemMax) {
       spill = sp;
       break;
     }
