@@ -42,6 +42,14 @@ def args_():
     p.add_argument("--states", type=int, default=1 << 20)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--launch", default="",
+                   help="ts,v,warps,global_ws: fixed rates-kernel mapping instead of the autotuner "
+                        "(profiling captures of one known kernel)")
+    p.add_argument("--reactors", type=int, default=2048,
+                   help="reactors of the 160-species integration workload (0: skip)")
+    p.add_argument("--integ-dt", type=float, default=2e-3,
+                   help="integration interval per reactor in seconds (2 ms: the workload; "
+                        "shorter only for bounded profiling captures)")
     return p.parse_args()
 
 
@@ -59,7 +67,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -141,6 +149,77 @@ def cpu_reference(files, T, P, Y, budget_s=12.0, nthreads=None):
                       f"({kind} exp) + restated SetupJacobianSparse, {nthreads} OpenMP threads"}
 
 
+def integration_bench(n_reactors, cpu=True, dt=2e-3):
+    """Reactors integrated/s on the 160-species / 900-reaction mechanism (2 ms
+    per reactor at rtol 1e-8, atol 1e-20) through the cfd_plugin API with host
+    arrays: the plain FP64 path (dense Newton inverse, direct solves) and the
+    FP32 form (single-precision inverse preconditioning an FP64 Krylov solve).
+    Each form is called twice on the same states; the second call, ordered by
+    the first call's per-reactor cost as the plugin does, is timed.  The CPU
+    oracle integrates a bounded sample of the same reactors on all host cores,
+    and its end states give the error of each GPU form."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    g = mechgen.generate(mechgen.SPECS["c3_160"])
+    out = {"metric": "reactors integrated/s at rtol 1e-8", "unit": "reactors/s",
+           "workload": f"160 species / 900 reactions, {n_reactors} constant-volume reactors "
+                       "(T U[700,2500] K, P U[1,100] atm, 1-4 fuel-like species), "
+                       f"{dt * 1e3:g} ms each, rtol 1e-8, atol 1e-20"}
+    with tempfile.TemporaryDirectory() as d:
+        mf, tf = g.write(d)
+        T, P, Y = mechgen.reactor_states(g, n_reactors, "c3", seed=11)
+        ends = {}
+        for name, fp32 in (("plain_fp64", 0), ("fp32_krylov", 1)):
+            p = Plugin(mf, tf, lu_fp32=fp32)
+            cost = p.set_aux_field("COST", np.zeros(n_reactors))
+            Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+            p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
+            Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+            t0 = time.perf_counter()
+            rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
+            wall = time.perf_counter() - t0
+            st = p.last_stats()
+            ends[name] = (Tg, Yg)
+            out[name] = {"value": n_reactors / wall, "wall_s": wall, "kernel_ms": st["kernel_ms"],
+                         "status": rc, "failed": st["nfailed"], "steps": st["nsteps"],
+                         "newton_iters": st["nnewt"], "rejected": st["nrej"],
+                         "factorizations": st["nlu"], "jacobians": st["njac"],
+                         "h2d_bytes": int(T.nbytes + P.nbytes + Y.nbytes),
+                         "d2h_bytes": int(T.nbytes + P.nbytes + Y.nbytes)}
+            p.close()
+        out["fp32_over_plain"] = out["fp32_krylov"]["value"] / out["plain_fp64"]["value"]
+        if cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import zerork_b200 as zb
+            import zrk_oracle as zo
+            pm = zb.Mechanism(mf, tf, device=False)
+            ot = _oracle_tables(pm, zo)
+            nth = os.cpu_count() or 1
+            m = min(n_reactors, 2 * nth)
+            t0 = time.perf_counter()
+            To, Po, Yo, so = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth)
+            dt = time.perf_counter() - t0
+            ok = so["status"] == 0
+            out["cpu_oracle"] = {"value": m / dt, "unit": "reactors/s", "cores": nth, "kind": "port",
+                                 "sample": f"first {m} of the {n_reactors} reactors, restated "
+                                           "BDF/Newton with dense LU (FP64), one reactor per thread",
+                                 "failed": int((~ok).sum())}
+            for name, (Tg, Yg) in ends.items():
+                out[name]["max_abs_dT_vs_oracle"] = float(np.abs(Tg[:m] - To)[ok].max())
+                out[name]["max_abs_dY_vs_oracle"] = float(np.abs(Yg[:m] - Yo)[ok].max())
+    return out
+
+
+def _oracle_tables(pm, zo):
+    """CPU oracle tables from the product loader's tables (the loader is pinned
+    bit-exact to the reference's own tables by the test suite)."""
+    d = pm.tables()
+    d.update(tot_reac=len(d["reac_spc"]), tot_prod=len(d["prod_spc"]), n_arr=len(d["arr_step"]),
+             n_keq=len(d["keq_step"]), n_tb=len(d["tb_fwd"]), n_fo=len(d["fo_fwd"]),
+             n_tb_eff=len(d["tb_spc"]), n_fo_eff=len(d["fo_eff_spc"]))
+    return zo.OracleTables(d)
+
+
 def run_reference_arm(a, rank, world):
     if rank != 0:
         return
@@ -215,7 +294,12 @@ def main():
         pm.rates_jac(Td, Pd, Yd, W, J, stream=sptr)
 
     # project autotuner: time every tile/warp mapping on the first 2^16 states
-    tuned, tuned_ms = pm.autotune(Td, Pd, Yd, W, J, n=min(n, 1 << 16), stream=sptr)
+    if a.launch:
+        ts, v, wp, gws = (int(x) for x in a.launch.split(","))
+        pm.set_launch(ts, v, wp, bool(gws), 0)
+        tuned_ms = None
+    else:
+        tuned, tuned_ms = pm.autotune(Td, Pd, Yd, W, J, n=min(n, 1 << 16), stream=sptr)
 
     for _ in range(a.warmup):
         step()
@@ -300,6 +384,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_reference(files, T, P, Y)
+    integ = None
+    if rank == 0 and world == 1 and a.reactors > 0:
+        integ = integration_bench(a.reactors, cpu=not a.no_cpu, dt=a.integ_dt)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "states/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
@@ -310,7 +397,7 @@ def main():
                            "global_states": world * n, "parallelism": f"shard{world}",
                            "l2": "inputs 445 MB + outputs 15 GB per step exceed L2; no flush",
                            "launch": pm.get_launch(), "autotune_sample_ms": tuned_ms},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "integration": integ,
                 "gpu_launches": a.steps, "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:
