@@ -1,0 +1,76 @@
+"""The oracle integrator (oracle/zrk_bdf.c) against an independent stiff
+integrator.
+
+CVODE is not vendored in the reference (SUNDIALS 5.8.0 is a download), so
+the oracle restates a published BDF; this cross-check integrates the same
+reactors with SciPy's BDF (solve_ivp, the Shampine-Reichelt NDF family) on
+the oracle's own right-hand side and Jacobian, both at tight tolerance, and
+requires the end states to agree within a few times the requested tolerance.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import oracle_tables, synth
+
+
+def _rhs_and_jac(ot, T0, P0, Y0):
+    L = ot.lib
+    kin = (C.c_char * 48)()
+    L.zo_kinetics_oracle(ot.ptr, C.cast(kin, C.c_void_p))
+    L.zo_reactor_new.restype = C.c_void_p
+    L.zo_reactor_new.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double]
+    L.zo_reactor_free.argtypes = [C.c_void_p]
+    L.zo_reactor_set_density.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p]
+    L.zo_cv_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.zo_jac_values.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                C.c_void_p]
+    r = L.zo_reactor_new(ot.ptr, kin, 1.0, 1e-30, 1e22)
+    Y0 = np.ascontiguousarray(Y0, dtype=np.float64)
+    L.zo_reactor_set_density(r, T0, P0, Y0.ctypes.data)
+    pat = ot.pat.contents
+    n, nnz = pat.n, pat.nnz
+    cp = np.ctypeslib.as_array(pat.col_ptr, (n + 1,)).copy()
+    ri = np.ctypeslib.as_array(pat.row_idx, (nnz,)).copy()
+
+    def f(t, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        out = np.zeros(n)
+        assert L.zo_cv_rhs(r, y.ctypes.data, out.ctypes.data) == 0
+        return out
+
+    def jac(t, y):
+        from scipy.sparse import csc_matrix
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        fy = f(t, y)
+        v = np.zeros(nnz)
+        L.zo_jac_values(r, ot.pat, y.ctypes.data, fy.ctypes.data, v.ctypes.data, None)
+        return csc_matrix((v, ri, cp), shape=(n, n))
+
+    return f, jac, lambda: L.zo_reactor_free(r)
+
+
+@pytest.mark.parametrize("idx", [0, 3, 7])
+def test_oracle_bdf_matches_scipy_bdf(idx, mech_dir):
+    scipy_integrate = pytest.importorskip("scipy.integrate")
+    import zerork_b200 as zb
+    from zerork_b200 import mechgen
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 8, "c1", seed=11)
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    dt, rtol, atol = 1e-3, 1e-10, 1e-22
+    To, Po, Yo, st = ot.solve(T[idx:idx + 1], P[idx:idx + 1], Y[idx:idx + 1], dt,
+                              rtol=rtol, atol=atol, max_steps=200000)
+    assert st["status"][0] == 0
+    f, jac, free = _rhs_and_jac(ot, T[idx], P[idx], Y[idx])
+    try:
+        y0 = np.concatenate([Y[idx], [T[idx]]])
+        sol = scipy_integrate.solve_ivp(f, (0.0, dt), y0, method="BDF", rtol=rtol, atol=atol,
+                                        jac=jac)
+    finally:
+        free()
+    assert sol.status == 0
+    ys = sol.y[:, -1]
+    assert abs(ys[-1] - To[0]) <= 1e-6 * To[0]
+    assert np.max(np.abs(ys[:-1] - Yo[0])) <= 1e-7
