@@ -10,7 +10,10 @@ tight-tolerance oracle run (rtol 1e-12), and the GPU error must be within
   max_k |Y_gpu - Y_tight| <= 50 * max_k |Y_oracle - Y_tight| + 1e-8
 per reactor: the oracle's own error at rtol 1e-8 sets the scale (two valid
 integrations at the same tolerance with different step sequences differ by
-a small multiple of it).
+a small multiple of it).  The per-reactor scale is floored at 10x the median
+oracle error over the batch, since a reactor whose oracle run happens to be
+far more accurate than the batch does not make a different valid
+integration of it less accurate.
 """
 import os
 
@@ -47,8 +50,9 @@ def _check_against_tight(ot, T, P, Y, dt, Tg, Yg):
     eg_T = np.abs(Tg - Tt)[ok]
     eo_Y = np.max(np.abs(Yo - Yt), axis=1)[ok]
     eg_Y = np.max(np.abs(Yg - Yt), axis=1)[ok]
-    assert np.all(eg_T <= 50 * eo_T + 1e-5 * Tt[ok]), (eg_T, eo_T)
-    assert np.all(eg_Y <= 50 * eo_Y + 1e-8), (eg_Y, eo_Y)
+    fT, fY = 10 * np.median(eo_T), 10 * np.median(eo_Y)
+    assert np.all(eg_T <= 50 * np.maximum(eo_T, fT) + 1e-5 * Tt[ok]), (eg_T, eo_T)
+    assert np.all(eg_Y <= 50 * np.maximum(eo_Y, fY) + 1e-8), (eg_Y, eo_Y)
     return eg_T, eg_Y
 
 

@@ -14,6 +14,7 @@
 #include <cstdint>
 
 #include "devmech.h"
+#include "mlp.h"
 #include "kinetics.h"
 
 namespace zrk {
@@ -28,6 +29,14 @@ struct LUDev {
   const int *diag_of_orig;              // original variable -> LU diagonal index
 };
 
+// Learned BDF predictor attached to the dense integrator: the network
+// (mlp.h) and the standardisation of its inputs and targets.
+struct PredDev {
+  MlpDev net;
+  const float *x_mu = nullptr, *x_sd = nullptr, *t_mu = nullptr, *t_sd = nullptr;
+  int enabled = 0;
+};
+
 struct IntegOpts {
   double rtol, atol, max_dt, nlscoef;
   int max_steps, max_retries;
@@ -35,6 +44,7 @@ struct IntegOpts {
   double Tref, mmf, lim, sqrt_ur;
   int lu_fp32;  // factor and apply the Newton matrix in FP32
   double eps_lin;  // Krylov tolerance: eps_lin * nlscoef / error constant (WRMS)
+  PredDev pred;    // learned predictor (dense integrator only; enabled = 0: off)
 };
 
 // Per-reactor statistics written by the kernel.

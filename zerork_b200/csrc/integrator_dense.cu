@@ -8,7 +8,7 @@ size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill) {
   const int n = m.nsp + 1;
   const int lda = (n % 2 == 1) ? n : n + 1;  // odd row stride: conflict-free column walks
   if (lda_out) *lda_out = lda;
-  size_t d = 128 + 3 * (size_t)m.nsp + 12 * (size_t)n + ((n + 1) / 2 + 1);
+  size_t d = 128 + 3 * (size_t)m.nsp + 12 * (size_t)n + ((n + 1) / 2 + 1) + kPredBuf;
   if (fp32) d += (kMaxl + 3) * (size_t)n;
   if (!(spill & 1)) d += m.nstep;
   if (!(spill & 2)) d += (kMaxOrder + 3) * (size_t)n;

@@ -26,6 +26,7 @@ constexpr double kMinFactor = 0.2;
 constexpr double kMaxFactor = 10.0;
 constexpr double kEtaKeep = 1.5;
 constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
+constexpr int kPredBuf = 256;  // widest predictor layer (padded)
 
 struct Smem {
   double *red;  // 128 slots: block sums [0, 33), pivot candidates [64, 112)
@@ -37,6 +38,7 @@ struct Smem {
   double *wlu;  // n: error-weight scale the stored inverse was formed with
   double *bs;   // n: scaled right-hand side
   double *V;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
+  float *mlp;   // learned predictor: two activation buffers of kPredBuf floats
 };
 
 // Sum over the CTA; every thread gets thread 0's total (deterministic).
@@ -499,6 +501,68 @@ __device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, doubl
   return rho < beta ? 1 : 2;
 }
 
+__device__ __forceinline__ float bf16_round(float x) { return __bfloat162float(__float2bfloat16(x)); }
+
+// Batch-one forward pass of the predictor network (mlp.cu's layers, the
+// same BF16 rounding of inputs and hidden activations, FP32 accumulation):
+// thread per output, bf16 weights read from global memory (L2-resident).
+// Returns the buffer holding the standardised outputs.
+__device__ float *mlp_forward_cta(const MlpDev &net, float *a, float *b) {
+  for (int l = 0; l < net.layers; ++l) {
+    const int K = net.dims[l], N = net.dims[l + 1];
+    const __nv_bfloat16 *W = net.w[l];
+    const bool hidden = l + 1 < net.layers;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+      float acc = 0.0f;
+#pragma unroll 8
+      for (int k = 0; k < K; ++k) acc = fmaf(a[k], __bfloat162float(W[(size_t)k * N + j]), acc);
+      const float z = acc + net.b[l][j];
+      b[j] = hidden ? bf16_round(z / (1.0f + expf(-z))) : z;
+    }
+    __syncthreads();
+    float *t = a;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Learned predictor (N3 form): the network's estimate of y(t + h) from the
+// last accepted state (row 0 of D) and h replaces the polynomial predictor
+// as the Newton starting iterate; ypred, psi and the error estimate keep the
+// polynomial predictor, so the error test judges the step exactly as
+// without the network.  Inputs: log10 of the clamped mass fractions,
+// (T - 1500 K) / 1000 K, log10(P / 1 bar), log10(h); targets: change of
+// log10 mass fraction and (T' - T) / 100 K, standardised.
+__device__ void predict_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v, double h) {
+  const int S = m.nsp, n = S + 1, tid = threadIdx.x, nt = blockDim.x;
+  const PredDev &p = o.pred;
+  const double *y0 = s.D;
+  double pw = 0.0;
+  for (int k = tid; k < S; k += nt) pw += y0[k] * m.inv_mw[k];
+  const double iw = block_sum(pw, s.red);
+  const double T = y0[S] * o.Tref;
+  const double P = kRuD * T * iw / v;
+  float *xa = s.mlp, *xb = s.mlp + kPredBuf;
+  for (int i = tid; i < p.net.dims[0]; i += nt) {
+    double f = 0.0;
+    if (i < S) f = log10(fmax(y0[i], 1e-30));
+    else if (i == S) f = (T - 1500.0) / 1000.0;
+    else if (i == S + 1) f = log10(fmax(P, 1e-300) / 1e5);
+    else if (i == S + 2) f = log10(h);
+    xa[i] = i < p.net.n_in ? bf16_round((float)((f - p.x_mu[i]) / p.x_sd[i])) : 0.0f;
+  }
+  __syncthreads();
+  const float *r = mlp_forward_cta(p.net, xa, xb);
+  for (int i = tid; i < n; i += nt) {
+    const double t = (double)r[i] * p.t_sd[i] + p.t_mu[i];
+    const double yi = i < S ? exp10(log10(fmax(y0[i], 1e-30)) + t) : (T + 100.0 * t) / o.Tref;
+    s.y[i] = yi;
+    s.d[i] = yi - s.ypred[i];
+  }
+  __syncthreads();
+}
+
 template <class LT, int NC>
 __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
                            double *J, double v, double t_end, double rtol, double atol,
@@ -535,7 +599,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   double h = fmin(100.0 * h0, h1);
   h = fmin(h, o.max_dt);
   h = fmin(h, t_end);
-  int q = 1, neq = 0, jac_current = 1, nsteps = 0;
+  int q = 1, neq = 0, jac_current = 1, nsteps = 0, pred_fail = 0;
   double c_lu = h / bc.alp[q], crate = 1.0;
   for (int i = tid; i < (kMaxOrder + 3) * n; i += nt) s.D[i] = 0.0;
   __syncthreads();
@@ -551,6 +615,11 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   while (t < t_end) {
     if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
+    // the learned predictor starts each step; any rejection falls back to
+    // the polynomial predictor for the rest of the step, and after two
+    // consecutive failed learned starts the reactor stops consulting the
+    // network for the rest of the attempt
+    bool use_pred = o.pred.enabled != 0 && pred_fail < 2;
     double safety = 0.9, err_norm = 0.0;
     while (!accepted) {
       if (h > o.max_dt) {
@@ -574,6 +643,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         s.d[i] = 0.0;
       }
       __syncthreads();
+      if (use_pred) predict_cta(m, o, s, v, h);
       const double c = h / bc.alp[q];
       if (fabs(c / c_lu - 1.0) > 0.3) {
         st.nlu++;
@@ -620,7 +690,10 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         }
         const double dn = sqrt(block_sum(a, s.red) / n);
         if (dnorm_old > 0.0) crate = fmax(0.3 * crate, dn / dnorm_old);
-        if (bc.econ[q] * dn * fmin(1.0, crate) <= o.nlscoef) {
+        // from a learned starting iterate, convergence is only declared on
+        // a contraction measured in this step (two iterations at least): the
+        // carried rate estimate describes the polynomial predictor's start
+        if (!(use_pred && it == 0) && bc.econ[q] * dn * fmin(1.0, crate) <= o.nlscoef) {
           conv = true;
           ++it;
           break;
@@ -629,6 +702,11 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         dnorm_old = dn;
       }
       if (!conv) {
+        if (use_pred) {  // the learned start failed: same step from the polynomial predictor
+          use_pred = false;
+          ++pred_fail;
+          continue;
+        }
         if (!jac_current) {
           st.nrhs++;
           if (rhs_cta(m, o, s, v, s.ypred, s.f0, false, nullptr)) { rc = -6; goto failed; }
@@ -655,12 +733,14 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
       err_norm = sqrt(block_sum(a, s.red) / n);
       if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
+        use_pred = false;
         const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D_cta(s.D, n, q, fac);
         h *= fac;
         st.nrej++;
         continue;
       }
+      if (use_pred) pred_fail = 0;  // the learned start converged and passed
       accepted = true;
       t = t_new;
     }
@@ -751,6 +831,8 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     s.V = p;
     p += (kMaxl + 3) * n;
   }
+  s.mlp = (float *)p;
+  p += kPredBuf;  // 2 * kPredBuf floats
   s.perm = (int *)p; p += (n + 1) / 2 + 1;
   s.A = p;
   Consts bc;

@@ -10,7 +10,9 @@
 #include <vector>
 
 #include "../../include/zerork_b200.h"
+#include "../../include/zerork_b200_predictor.h"
 #include "../../include/zerork_cfd_plugin.h"
+#include "mlp.h"
 #include "solver.h"
 
 struct zerork_handle_impl {
@@ -26,6 +28,9 @@ struct zerork_handle_impl {
   int *reactor_ids = nullptr;
   zrk::SolveStatsTotals last;
   std::string last_error;
+  zrk::PredDev pred{};       // learned predictor (network owned by the caller)
+  float *pred_norm = nullptr;  // device copy of the standardisation vectors
+  ~zerork_handle_impl() { cudaFree(pred_norm); }
 };
 
 namespace {
@@ -212,6 +217,7 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
   o.warps_per_cta = I["gpu_warps_per_cta"];
   o.method = I["gpu_method"];
   o.threads = I["gpu_threads"];
+  o.pred = h->pred;
   // aux fields owned by the handle when the caller gave none
   // (zerork_reactor_manager.cpp:502-519)
   const int n = n_reactors;
@@ -325,6 +331,46 @@ zerork_status_t zerork_reactor_free(zerork_handle h) {
 
 // Totals of the last solve call: steps, rejected steps, Newton iterations,
 // Jacobians, factorizations, right-hand sides, failed reactors; kernel ms.
+int zrk_plugin_set_predictor(zerork_handle h, zrk_mlp_t net, const float *x_mu, const float *x_sd,
+                             const float *t_mu, const float *t_sd) {
+  if (!h) return ZRK_ERR_INVALID_HANDLE;
+  if (!net) {
+    h->pred.enabled = 0;
+    return ZRK_OK;
+  }
+  if (!x_mu || !x_sd || !t_mu || !t_sd) return ZRK_ERR_INVALID_POINTER;
+  if (ensure_mechanism(h) != ZERORK_STATUS_SUCCESS) return ZRK_ERR_PARSE;
+  const zrk::MlpDev d = reinterpret_cast<zrk::Mlp *>(net)->device_view();
+  const int nsp = h->solver->nsp();
+  if (d.n_in != nsp + 3 || d.n_out != nsp + 1) {
+    h->last_error = "predictor sizes must be nsp + 3 inputs and nsp + 1 outputs";
+    return ZRK_ERR_INVALID_ARGUMENT;
+  }
+  for (int l = 0; l <= d.layers; ++l)
+    if (d.dims[l] > 256) {
+      h->last_error = "predictor layers wider than 256 are not supported by the integrator";
+      return ZRK_ERR_INVALID_ARGUMENT;
+    }
+  const size_t ni = d.n_in, no = d.n_out;
+  std::vector<float> buf;
+  buf.insert(buf.end(), x_mu, x_mu + ni);
+  buf.insert(buf.end(), x_sd, x_sd + ni);
+  buf.insert(buf.end(), t_mu, t_mu + no);
+  buf.insert(buf.end(), t_sd, t_sd + no);
+  cudaFree(h->pred_norm);
+  h->pred_norm = nullptr;
+  if (cudaMalloc(&h->pred_norm, buf.size() * sizeof(float)) != cudaSuccess ||
+      cudaMemcpy(h->pred_norm, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess)
+    return ZRK_ERR_CUDA;
+  h->pred.net = d;
+  h->pred.x_mu = h->pred_norm;
+  h->pred.x_sd = h->pred_norm + ni;
+  h->pred.t_mu = h->pred_norm + 2 * ni;
+  h->pred.t_sd = h->pred_norm + 2 * ni + no;
+  h->pred.enabled = 1;
+  return ZRK_OK;
+}
+
 int zrk_plugin_last_stats(zerork_handle h, long *totals7, float *kernel_ms) {
   if (!h) return ZRK_ERR_INVALID_HANDLE;
   if (totals7) {

@@ -167,6 +167,8 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.max_dt = o.max_dt;
   io.nlscoef = o.nlscoef;
   io.eps_lin = o.eps_lin;
+  io.pred = o.pred;
+  if (io.pred.enabled && method != 1) io.pred.enabled = 0;  // dense integrator only
   io.max_steps = o.max_steps;
   io.max_retries = std::max(1, o.max_retries);
   io.retry_atol_factor = o.retry_atol;

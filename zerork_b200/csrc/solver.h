@@ -31,6 +31,7 @@ struct SolveOptions {
   int warps_per_cta = 0;  // 0 = automatic
   int method = 0;         // 0 automatic, 1 CTA dense block, 2 warp sparse LU
   int threads = 0;        // CTA size of the dense method (0 = automatic)
+  PredDev pred{};         // learned predictor (dense method only)
 };
 
 struct SolveStatsTotals {

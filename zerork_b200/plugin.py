@@ -50,6 +50,7 @@ def plugin_lib():
         L.zerork_reactor_set_reactor_ids.argtypes = [vp, vp]
         L.zerork_reactor_free.argtypes = [vp]
         L.zrk_plugin_last_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_float)]
+        L.zrk_plugin_set_predictor.argtypes = [vp, vp, vp, vp, vp, vp]
         _bound = True
     return L
 
@@ -136,6 +137,21 @@ class Plugin:
         if rc != 0 and (raise_on_fail or rc != 7):
             raise PluginError(rc, "zerork_reactor_solve")
         return rc
+
+    def set_predictor(self, net, x_scaler=None, t_scaler=None):
+        """Attach a trained predictor network (zerork_b200.predictor.Mlp) with
+        its input/target standardisation; net=None detaches it."""
+        if net is None:
+            self.check(self.L.zrk_plugin_set_predictor(self.h, None, None, None, None, None),
+                       "set_predictor")
+            self._keep.pop("predictor", None)
+            return
+        arrs = [np.ascontiguousarray(a, dtype=np.float32)
+                for a in (x_scaler.mu, x_scaler.sd, t_scaler.mu, t_scaler.sd)]
+        self._keep["predictor"] = (net, arrs)
+        rc = self.L.zrk_plugin_set_predictor(self.h, net.h, *[a.ctypes.data for a in arrs])
+        if rc != 0:
+            raise PluginError(99, "set_predictor: " + _lib().zrk_last_error().decode())
 
     def last_stats(self):
         t = (C.c_long * 7)()
