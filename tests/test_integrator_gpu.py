@@ -56,7 +56,7 @@ def _check_against_tight(ot, T, P, Y, dt, Tg, Yg):
     return eg_T, eg_Y
 
 
-@pytest.mark.parametrize("fp32,method", [(0, 1), (1, 1), (0, 2)])
+@pytest.mark.parametrize("fp32,method", [(0, 1), (1, 1), (0, 2), (1, 2)])
 def test_c1_end_states(gpu, fp32, method, mech_dir):
     from zerork_b200 import mechgen
     import zerork_b200 as zb
@@ -81,6 +81,20 @@ def test_c3_subset_end_states(gpu, fp32, mech_dir):
     rc, Tg, Pg, Yg, p = _solve(mf, tf, T, P, Y, 2e-4, lu_fp32=fp32)
     ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
     _check_against_tight(ot, T, P, Y, 2e-4, Tg, Yg)
+
+
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_c4_subset_end_states(gpu, fp32, mech_dir):
+    """650 species: the dense block does not fit, the warp-level sparse LU path
+    runs (FP32: the factor preconditions an FP64 Krylov solve)."""
+    from zerork_b200 import mechgen
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c4_650", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 6, "c4", seed=11)
+    rc, Tg, Pg, Yg, p = _solve(mf, tf, T, P, Y, 5e-4, lu_fp32=fp32)
+    assert rc == 0
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    _check_against_tight(ot, T, P, Y, 5e-4, Tg, Yg)
 
 
 def test_failure_leaves_state_and_reports(gpu, mech_dir):

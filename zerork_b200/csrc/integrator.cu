@@ -150,13 +150,24 @@ __device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
   return 0;
 }
 
-// P = I - cJ into the LU storage, then left-looking factorization in place.
+// Pw = W^-1 (I - cJ) W into the LU storage, W = diag(scale) the error
+// weights of the current step (entry (i, j) is P_ij scale_j / scale_i, the
+// Jacobian of relative changes: far better balanced than P for species
+// spanning 20 decades of mass fraction), then left-looking factorization in
+// place.  wsc receives the scale the factor was formed with.
 template <class LT>
-__device__ int lu_factor_warp(const LUDev &lu, const double *J, int jnnz, double c, LT *LU, LT *x,
-                              int lane) {
+__device__ int lu_factor_warp(const DevMech &m, const LUDev &lu, const double *J, double c,
+                              const double *scale, double *wsc, LT *LU, LT *x, int lane) {
   for (int p = lane; p < lu.nnz; p += 32) LU[p] = (LT)0;
+  for (int i = lane; i < lu.n; i += 32) wsc[i] = scale[i];
   __syncwarp();
-  for (int k = lane; k < jnnz; k += 32) LU[lu.jac_to_lu[k]] = (LT)(-c * J[k]);
+  for (int i = lane; i < lu.n; i += 32) {  // Jacobian row i from the row-wise view
+    const double ci = -c / scale[i];
+    for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) {
+      const int k = m.jr_kk[q];
+      LU[lu.jac_to_lu[k]] = (LT)(ci * J[k] * scale[m.jr_col[q]]);
+    }
+  }
   __syncwarp();
   for (int i = lane; i < lu.n; i += 32) LU[lu.diag_of_orig[i]] += (LT)1;
   __syncwarp();
@@ -206,6 +217,18 @@ __device__ void lu_solve_warp(const LUDev &lu, const LT *LU, LT *x, int lane) {
   }
 }
 
+// out = (I - c_lu J)^{-1} r from the scaled factor: W LU^-1 (W^-1 r), with
+// the permuted solve vector x in shared memory.
+template <class LT>
+__device__ void precond_warp(const LUDev &lu, const LT *LU, LT *x, const double *wsc, const double *r,
+                             double *out, int lane) {
+  for (int i = lane; i < lu.n; i += 32) x[lu.iperm[i]] = (LT)(r[i] / wsc[i]);
+  __syncwarp();
+  lu_solve_warp<LT>(lu, LU, x, lane);
+  for (int i = lane; i < lu.n; i += 32) out[i] = (double)x[lu.iperm[i]] * wsc[i];
+  __syncwarp();
+}
+
 // D[0..order] <- (R(factor) U)^T D[0..order], lanes over the n columns.
 __device__ void change_D(double *D, int n, int order, double fac, int lane) {
   double R[kMaxOrder + 1][kMaxOrder + 1], U[kMaxOrder + 1][kMaxOrder + 1];
@@ -238,7 +261,119 @@ __device__ void change_D(double *D, int n, int order, double fac, int lane) {
 
 struct Vecs {
   double *D, *y, *f, *f0, *ypred, *psi, *d, *scale, *tmp, *J;
+  double *wsc;  // scale the stored factor was formed with
+  double *K;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
 };
+
+constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
+
+// Left-preconditioned GMRES for (I - cJ) x = b on one warp, the Newton
+// system of the FP32 path: the operator is applied in FP64 from the stored
+// sparse Jacobian, the FP32 factor only preconditions, in the error-weighted
+// coordinates; SPGMR's method (modified Gram-Schmidt, no restarts, x0 = 0,
+// converged when the preconditioned residual's weighted 2-norm is <= delta),
+// as the reference plugin drives it through CVODE (solver_cvode.cpp:119-141,
+// 201-212), restated from Saad and Schultz, SIAM J. Sci. Stat. Comput. 7
+// (1986) 856-869.  Every lane keeps the same Hessenberg matrix.  Returns 0
+// when converged, 1 otherwise.
+template <class LT>
+__device__ int gmres_warp(const DevMech &m, const LUDev &lu, const Vecs &V, const LT *LU, LT *x, double c,
+                          double delta, const double *b, double *xo, int lane) {
+  const int n = lu.n;
+  double *Kv = V.K, *u = V.K + (kMaxl + 1) * n, *z = u + n;
+  precond_warp<LT>(lu, LU, x, V.wsc, b, z, lane);
+  double a = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double t = z[i] / V.scale[i];
+    Kv[i] = t;
+    a += t * t;
+  }
+  const double beta = sqrt(wsum(a));
+  if (!isfinite(beta)) return 1;
+  if (beta <= delta) {
+    for (int i = lane; i < n; i += 32) xo[i] = 0.0;
+    __syncwarp();
+    return 0;
+  }
+  double H[kMaxl + 1][kMaxl], cs[kMaxl], sn[kMaxl], g[kMaxl + 1], yk[kMaxl];
+  g[0] = beta;
+  for (int i = lane; i < n; i += 32) Kv[i] /= beta;
+  int nl = 0;
+  bool conv = false;
+  for (int l = 0; l < kMaxl; ++l) {
+    const double *vl = Kv + l * n;
+    double *w = Kv + (l + 1) * n;
+    for (int i = lane; i < n; i += 32) u[i] = vl[i] * V.scale[i];
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {  // (I - cJ) u, row i
+      double jx = 0.0;
+      for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) jx += V.J[m.jr_kk[q]] * u[m.jr_col[q]];
+      z[i] = u[i] - c * jx;
+    }
+    __syncwarp();
+    precond_warp<LT>(lu, LU, x, V.wsc, z, z, lane);
+    for (int i = lane; i < n; i += 32) w[i] = z[i] / V.scale[i];
+    __syncwarp();
+    for (int k = 0; k <= l; ++k) {  // modified Gram-Schmidt
+      const double *vk = Kv + k * n;
+      double d = 0.0;
+      for (int i = lane; i < n; i += 32) d += w[i] * vk[i];
+      const double h = wsum(d);
+      H[k][l] = h;
+      for (int i = lane; i < n; i += 32) w[i] -= h * vk[i];
+    }
+    double d2 = 0.0;
+    for (int i = lane; i < n; i += 32) d2 += w[i] * w[i];
+    const double hn = sqrt(wsum(d2));
+    for (int k = 0; k < l; ++k) {
+      const double h0 = H[k][l], h1 = H[k + 1][l];
+      H[k][l] = cs[k] * h0 + sn[k] * h1;
+      H[k + 1][l] = -sn[k] * h0 + cs[k] * h1;
+    }
+    const double a0 = H[l][l];
+    double cc, ss;
+    if (hn == 0.0) {
+      cc = 1.0;
+      ss = 0.0;
+    } else if (fabs(hn) > fabs(a0)) {
+      const double t = a0 / hn;
+      ss = 1.0 / sqrt(1.0 + t * t);
+      cc = ss * t;
+    } else {
+      const double t = hn / a0;
+      cc = 1.0 / sqrt(1.0 + t * t);
+      ss = cc * t;
+    }
+    H[l][l] = cc * a0 + ss * hn;
+    cs[l] = cc;
+    sn[l] = ss;
+    g[l + 1] = -ss * g[l];
+    g[l] = cc * g[l];
+    const double rho = fabs(g[l + 1]);
+    nl = l + 1;
+    if (hn > 0.0)
+      for (int i = lane; i < n; i += 32) w[i] /= hn;
+    __syncwarp();
+    if (!isfinite(rho)) return 1;
+    if (rho <= delta) {
+      conv = true;
+      break;
+    }
+    if (hn == 0.0) break;
+  }
+  for (int k = nl - 1; k >= 0; --k) {
+    double t = g[k];
+    for (int j = k + 1; j < nl; ++j) t -= H[k][j] * yk[j];
+    yk[k] = t / H[k][k];
+  }
+  for (int i = lane; i < n; i += 32) {
+    double acc = 0.0;
+    for (int k = 0; k < nl; ++k) acc += yk[k] * Kv[k * n + i];
+    xo[i] = acc * V.scale[i];
+  }
+  __syncwarp();
+  return conv ? 0 : 1;
+}
 
 __device__ __forceinline__ double wrms_scaled(const double *x, const double *s, int n, int lane) {
   double a = 0.0;
@@ -257,7 +392,6 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
                            const Warp &w, const Vecs &V, LT *LU, double v, double t_end,
                            double rtol, double atol, ReactorStats &st, int lane, double &t_done) {
   const int n = m.nsp + 1;
-  const int jnnz = m.nnz;
   LT *x = (LT *)w.X;
   double t = 0.0;
   int rc = 0;
@@ -295,7 +429,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   st.njac++;
   if (jac_warp(m, o, w, v, V.y, V.f0, V.J, V.tmp, V.d, lane)) { rc = -2; goto failed; }
   st.nlu++;
-  if (lu_factor_warp<LT>(lu, V.J, jnnz, c_lu, LU, x, lane)) { rc = -3; goto failed; }
+  if (lu_factor_warp<LT>(m, lu, V.J, c_lu, V.scale, V.wsc, LU, x, lane)) { rc = -3; goto failed; }
   while (t < t_end) {
     if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
@@ -327,7 +461,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         st.nlu++;
         c_lu = c;
         crate = 1.0;
-        if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) { rc = -3; goto failed; }
+        if (lu_factor_warp<LT>(m, lu, V.J, c, V.scale, V.wsc, LU, x, lane)) { rc = -3; goto failed; }
       }
       const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
       bool conv = false;
@@ -342,13 +476,22 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         if (it == 0)
           for (int i = lane; i < n; i += 32) V.f0[i] = V.f[i];
         st.nnewt++;
-        for (int i = lane; i < n; i += 32)
-          x[lu.iperm[i]] = (LT)(c * V.f[i] - V.psi[i] - V.d[i]);
+        for (int i = lane; i < n; i += 32) V.tmp[i] = c * V.f[i] - V.psi[i] - V.d[i];
         __syncwarp();
-        lu_solve_warp<LT>(lu, LU, x, lane);
+        double gs = gscale;
+        if constexpr (sizeof(LT) == sizeof(float)) {
+          // FP32 factor as the preconditioner of an FP64 Krylov solve with
+          // tolerance eps_lin * nlscoef / error constant (WRMS); every solve
+          // must converge (see integrator_dense.cuh)
+          const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
+          if (gmres_warp<LT>(m, lu, V, LU, x, c, delta, V.tmp, V.tmp, lane) != 0) break;
+          gs = 1.0;
+        } else {
+          precond_warp<LT>(lu, LU, x, V.wsc, V.tmp, V.tmp, lane);
+        }
         double a = 0.0;
         for (int i = lane; i < n; i += 32) {
-          const double dy = (double)x[lu.iperm[i]] * gscale;
+          const double dy = V.tmp[i] * gs;
           V.y[i] += dy;
           V.d[i] += dy;
           const double tt = dy / V.scale[i];
@@ -375,7 +518,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
           st.nlu++;
           c_lu = c;
           crate = 1.0;
-          if (lu_factor_warp<LT>(lu, V.J, jnnz, c, LU, x, lane)) { rc = -3; goto failed; }
+          if (lu_factor_warp<LT>(m, lu, V.J, c, V.scale, V.wsc, LU, x, lane)) { rc = -3; goto failed; }
           continue;
         }
         change_D(V.D, n, q, 0.5, lane);
@@ -496,6 +639,8 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     V.scale = V.d + n;
     V.tmp = V.scale + n;
     V.J = V.tmp + n;
+    V.wsc = V.J + m.nnz;
+    V.K = V.wsc + n;
     LT *LU = (LT *)a.lu + (size_t)r * a.lu_stride;
     // InitializeState (reactor_constant_volume_cpu.cpp:15-41)
     const double T0 = a.T[r], P0 = a.P[r];
@@ -555,7 +700,7 @@ size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem) 
 
 long integ_state_doubles(const DevMech &m, const LUDev &lu) {
   const long n = m.nsp + 1;
-  return (kMaxOrder + 3) * n + 8 * n + m.nnz;
+  return (kMaxOrder + 3) * n + 8 * n + m.nnz + n + (kMaxl + 3) * n;
 }
 
 cudaError_t launch_integrate(const DevMech &m, const LUDev &lu, const IntegOpts &o,
