@@ -136,6 +136,22 @@ int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, co
 struct zerork_handle_impl;
 int zrk_plugin_last_stats(struct zerork_handle_impl *h, long *totals7, float *kernel_ms);
 
+/* Every zerork_reactor_solve call runs as one CUDA graph (copies in, work
+ * queue reset, the persistent integration kernel, copies out), captured when
+ * the call's configuration (reactor count, launch mapping, options, dt)
+ * changes and replayed otherwise.  Counts of captures and launches so far.
+ * No counterpart in the reference. */
+int zrk_plugin_graph_stats(struct zerork_handle_impl *h, long *captures, long *launches);
+
+/* Integrator launch-mapping autotuner: times the dense path's CTA sizes
+ * (128/256/512 threads) or the sparse path's warps per CTA (4/8/12) on a
+ * sample of the given reactors (at most 2 per SM) over dt / 20, keeps the
+ * fastest as the handle's gpu_threads / gpu_warps_per_cta option and
+ * returns it with its kernel time.  The inputs are not modified.  No
+ * counterpart in the reference (its GPU path has fixed launch sizes). */
+int zrk_plugin_autotune(struct zerork_handle_impl *h, int n, double dt, const double *T,
+                        const double *P, const double *mass_fractions, int *best, float *best_ms);
+
 #ifdef __cplusplus
 }
 #endif

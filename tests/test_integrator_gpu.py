@@ -126,7 +126,27 @@ def test_cost_and_temperature_delta_fields(gpu, mech_dir):
     assert np.all(cost > 0)
     d = Tg - T
     assert np.allclose(tdel, np.where(d < 2.0, 0.0, d))
-    # second call reuses the cost ordering and gives the same answer
+    # second call reuses the cost ordering and gives the same answer, replaying
+    # the captured graph of the first call
     T2, P2, Y2 = T.copy(), P.copy(), Y.copy()
     assert p.solve(1e-3, T2, P2, Y2) == 0
     assert np.array_equal(T2, Tg) and np.array_equal(Y2, Yg)
+    assert p.graph_stats() == {"captures": 1, "launches": 2}
+    # a different interval is a different graph
+    T3, P3, Y3 = T.copy(), P.copy(), Y.copy()
+    assert p.solve(5e-4, T3, P3, Y3) == 0
+    assert p.graph_stats() == {"captures": 2, "launches": 3}
+
+
+def test_integrator_autotune(gpu, mech_dir):
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 64, "c1", seed=6)
+    p = Plugin(mf, tf)
+    T0, Y0 = T.copy(), Y.copy()
+    best, ms = p.autotune(1e-3, T, P, Y)
+    assert best in (128, 256, 512) and ms > 0
+    assert p.get_int("gpu_threads") == best
+    assert np.array_equal(T, T0) and np.array_equal(Y, Y0)
+    assert p.solve(1e-3, T, P, Y) == 0

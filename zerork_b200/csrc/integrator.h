@@ -35,6 +35,7 @@ struct PredDev {
   MlpDev net;
   const float *x_mu = nullptr, *x_sd = nullptr, *t_mu = nullptr, *t_sd = nullptr;
   int enabled = 0;
+  int reserved = 0;  // no implicit padding: the struct's bytes key captured graphs
 };
 
 struct IntegOpts {

@@ -187,16 +187,8 @@ zerork_status_t zerork_reactor_load_mechanism(zerork_handle h) {
   return ensure_mechanism(h);
 }
 
-zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const double dt,
-                                     const int n_reactors, double *T, double *P, double *mf,
-                                     zerork_handle h) {
-  (void)n_cycle;
-  (void)time;
-  if (!h) return ZERORK_STATUS_INVALID_HANDLE;
-  zerork_status_t f = ensure_mechanism(h);
-  if (f != ZERORK_STATUS_SUCCESS) return f;
-  if (n_reactors <= 0) return ZERORK_STATUS_SUCCESS;
-  if (!T || !P || !mf) return ZERORK_STATUS_INVALID_POINTER;
+// Solver options from the handle's option maps (names as the reference's).
+static zrk::SolveOptions options_of(zerork_handle_impl *h) {
   auto &I = h->iopt;
   auto &D = h->dopt;
   zrk::SolveOptions o;
@@ -218,6 +210,21 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
   o.method = I["gpu_method"];
   o.threads = I["gpu_threads"];
   o.pred = h->pred;
+  return o;
+}
+
+zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const double dt,
+                                     const int n_reactors, double *T, double *P, double *mf,
+                                     zerork_handle h) {
+  (void)n_cycle;
+  (void)time;
+  if (!h) return ZERORK_STATUS_INVALID_HANDLE;
+  zerork_status_t f = ensure_mechanism(h);
+  if (f != ZERORK_STATUS_SUCCESS) return f;
+  if (n_reactors <= 0) return ZERORK_STATUS_SUCCESS;
+  if (!T || !P || !mf) return ZERORK_STATUS_INVALID_POINTER;
+  auto &D = h->dopt;
+  zrk::SolveOptions o = options_of(h);
   // aux fields owned by the handle when the caller gave none
   // (zerork_reactor_manager.cpp:502-519)
   const int n = n_reactors;
@@ -331,6 +338,62 @@ zerork_status_t zerork_reactor_free(zerork_handle h) {
 
 // Totals of the last solve call: steps, rejected steps, Newton iterations,
 // Jacobians, factorizations, right-hand sides, failed reactors; kernel ms.
+int zrk_plugin_graph_stats(zerork_handle h, long *captures, long *launches) {
+  if (!h) return ZRK_ERR_INVALID_HANDLE;
+  if (captures) *captures = h->solver ? h->solver->graph_captures : 0;
+  if (launches) *launches = h->solver ? h->solver->graph_launches : 0;
+  return ZRK_OK;
+}
+
+// Integrator launch-mapping autotuner: the CTA size of the dense-block path
+// (128, 256, 512 threads) or the warps per CTA of the sparse path (4, 8, 12),
+// each timed on the same sample of the caller's reactors over a short
+// interval; the fastest becomes the handle's gpu_threads / gpu_warps_per_cta.
+int zrk_plugin_autotune(zerork_handle h, int n, double dt, const double *T, const double *P,
+                        const double *mf, int *best, float *best_ms) {
+  if (!h) return ZRK_ERR_INVALID_HANDLE;
+  if (!T || !P || !mf) return ZRK_ERR_INVALID_POINTER;
+  if (n <= 0 || !(dt > 0.0)) return ZRK_ERR_INVALID_ARGUMENT;
+  if (ensure_mechanism(h) != ZERORK_STATUS_SUCCESS) return ZRK_ERR_PARSE;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int ns = h->solver->nsp();
+  const int m = std::min(n, 2 * sms);
+  const double dtt = dt / 20.0;
+  zrk::SolveOptions o = options_of(h);
+  int method = o.method;
+  // probe which path runs: the dense path sets gpu_threads, the sparse path warps
+  std::vector<double> T1(T, T + m), P1(P, P + m), Y1(mf, mf + (size_t)m * ns);
+  zrk::SolveStatsTotals tot;
+  if (h->solver->solve(o, m, dtt, T1.data(), P1.data(), Y1.data(), ns, nullptr, nullptr, nullptr, 2.0,
+                       nullptr, &tot) < 0)
+    return ZRK_ERR_CUDA;
+  method = tot.method;
+  const std::vector<int> cand = method == 1 ? std::vector<int>{128, 256, 512} : std::vector<int>{4, 8, 12};
+  float bms = 1e30f;
+  int bc = cand.back();
+  for (int c : cand) {
+    zrk::SolveOptions oc = o;
+    if (method == 1) oc.threads = c;
+    else oc.warps_per_cta = c;
+    std::copy(T, T + m, T1.begin());
+    std::copy(P, P + m, P1.begin());
+    std::copy(mf, mf + (size_t)m * ns, Y1.begin());
+    if (h->solver->solve(oc, m, dtt, T1.data(), P1.data(), Y1.data(), ns, nullptr, nullptr, nullptr, 2.0,
+                         nullptr, &tot) < 0)
+      continue;
+    if (tot.kernel_ms < bms) {
+      bms = tot.kernel_ms;
+      bc = c;
+    }
+  }
+  h->iopt[method == 1 ? "gpu_threads" : "gpu_warps_per_cta"] = bc;
+  if (best) *best = bc;
+  if (best_ms) *best_ms = bms;
+  return ZRK_OK;
+}
+
 int zrk_plugin_set_predictor(zerork_handle h, zrk_mlp_t net, const float *x_mu, const float *x_sd,
                              const float *t_mu, const float *t_sd) {
   if (!h) return ZRK_ERR_INVALID_HANDLE;

@@ -49,6 +49,8 @@ ReactorSolver::ReactorSolver(const std::string &mech, const std::string &therm) 
 }
 
 ReactorSolver::~ReactorSolver() {
+  if (graph_) cudaGraphExecDestroy(graph_);
+  cudaFreeHost(hT_); cudaFreeHost(hP_); cudaFreeHost(hY_); cudaFreeHost(horder_); cudaFreeHost(hstats_);
   cudaFree(lu_blob_);
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_); cudaFree(drop_);
@@ -61,6 +63,13 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   if (n <= cap_ && fp32 == cap_fp32_) return cudaSuccess;
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_);
+  cudaFreeHost(hT_); cudaFreeHost(hP_); cudaFreeHost(hY_); cudaFreeHost(horder_); cudaFreeHost(hstats_);
+  hT_ = hP_ = hY_ = nullptr;
+  horder_ = nullptr;
+  hstats_ = nullptr;
+  if (graph_) cudaGraphExecDestroy(graph_);
+  graph_ = nullptr;
+  graph_key_.clear();
   dT_ = dP_ = dY_ = dv_ = dstate_ = nullptr;
   dlu_ = nullptr;
   dstats_ = nullptr;
@@ -81,6 +90,11 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   if ((e = cudaMalloc(&dstats_, cap * sizeof(ReactorStats))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&dorder_, cap * sizeof(int))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&dhead_, sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hT_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hP_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hY_, cap * S * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&horder_, cap * sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hstats_, cap * sizeof(ReactorStats))) != cudaSuccess) return e;
   cap_ = cap;
   cap_fp32_ = fp32;
   return cudaSuccess;
@@ -102,8 +116,11 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   if (o.sort_reactors && cost)  // longest previous cost first (work queue)
     std::stable_sort(order.begin(), order.end(),
                      [&](int a, int b) { return std::fabs(cost[a]) > std::fabs(cost[b]); });
-  std::vector<double> Y((size_t)n * S), T0(T, T + n);
+  std::vector<double> T0(T, T + n);
+  double *Y = hY_;  // packed reactor-major mass fractions in pinned staging
   for (int r = 0; r < n; ++r) std::memcpy(&Y[(size_t)r * S], mf + (size_t)r * stride, S * sizeof(double));
+  std::memcpy(hT_, T, n * sizeof(double));
+  std::memcpy(hP_, P, n * sizeof(double));
   const DevMech &m = dm_->view();
   const size_t kSmemMax = 227 * 1024;
   // dense block in shared memory, spilling the rates of progress and then the
@@ -162,6 +179,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     }
   }
   IntegOpts io;
+  std::memset(&io, 0, sizeof(io));  // padding too: the bytes key the captured graph
   io.rtol = o.rtol;
   io.atol = o.atol;
   io.max_dt = o.max_dt;
@@ -179,6 +197,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.sqrt_ur = std::sqrt(2.2204460492503131e-16);
   io.lu_fp32 = o.lu_fp32 ? 1 : 0;
   IntegArgs a;
+  std::memset(&a, 0, sizeof(a));
   a.n_reactors = n;
   a.order = dorder_;
   a.queue_head = dhead_;
@@ -194,41 +213,73 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   a.stats = dstats_;
   a.rop_scratch = drop_;
   cudaStream_t s = stream_;
-  if ((e = cudaMemcpyAsync(dT_, T, n * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(dP_, P, n * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(dY_, Y.data(), Y.size() * sizeof(double), cudaMemcpyHostToDevice, s)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(dorder_, order.data(), n * sizeof(int), cudaMemcpyHostToDevice, s)) !=
-          cudaSuccess ||
-      (e = cudaMemsetAsync(dhead_, 0, sizeof(int), s)) != cudaSuccess) {
-    last_error = std::string("H2D: ") + cudaGetErrorString(e);
-    return -1;
-  }
+  std::memcpy(horder_, order.data(), n * sizeof(int));
   if (method == 1) {
     a.state = dstate_;
     a.state_stride = m.nnz;
   }
-  cudaEventRecord(ev0_, s);
-  e = method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)
-                  : launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s);
-  cudaEventRecord(ev1_, s);
-  if (e != cudaSuccess) {
-    last_error = std::string("integrate launch: ") + cudaGetErrorString(e);
-    return -1;
+  // The whole call (copies in, queue reset, the persistent kernel between
+  // two timing events, copies out) is one CUDA graph, captured once per
+  // configuration and replayed while nothing it depends on changes.
+  std::vector<unsigned char> key;
+  auto put_key = [&](const void *p, size_t b) {
+    key.insert(key.end(), (const unsigned char *)p, (const unsigned char *)p + b);
+  };
+  const int kv[9] = {n, method, dthreads, dctas, spill, W, ctas, rop_smem ? 1 : 0, S};
+  put_key(kv, sizeof(kv));
+  put_key(&io, sizeof(io));
+  put_key(&a, sizeof(a));
+  if (!graph_ || key != graph_key_) {
+    if (graph_) cudaGraphExecDestroy(graph_);
+    graph_ = nullptr;
+    graph_key_.clear();
+    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
+      last_error = std::string("graph capture: ") + cudaGetErrorString(e);
+      return -1;
+    }
+    cudaError_t ce = cudaSuccess;
+    auto q = [&](cudaError_t r) {
+      if (ce == cudaSuccess) ce = r;
+    };
+    q(cudaMemcpyAsync(dT_, hT_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaMemcpyAsync(dP_, hP_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaMemcpyAsync(dorder_, horder_, n * sizeof(int), cudaMemcpyHostToDevice, s));
+    q(cudaMemsetAsync(dhead_, 0, sizeof(int), s));
+    q(cudaEventRecordWithFlags(ev0_, s, cudaEventRecordExternal));  // a timing node in the graph
+    q(method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)
+                  : launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s));
+    q(cudaEventRecordWithFlags(ev1_, s, cudaEventRecordExternal));
+    q(cudaMemcpyAsync(hT_, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaMemcpyAsync(hP_, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaMemcpyAsync(hY_, dY_, (size_t)n * S * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaMemcpyAsync(hstats_, dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s));
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(s, &g);
+    if (ce == cudaSuccess) ce = ee;
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&graph_, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      graph_ = nullptr;
+      last_error = std::string("graph capture: ") + cudaGetErrorString(ce);
+      return -1;
+    }
+    graph_key_ = key;
+    ++graph_captures;
   }
-  std::vector<ReactorStats> st(n);
-  if ((e = cudaMemcpyAsync(T, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(P, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(Y.data(), dY_, Y.size() * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(st.data(), dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s)) !=
-          cudaSuccess ||
-      (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+  if ((e = cudaGraphLaunch(graph_, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess) {
     last_error = std::string("integration: ") + cudaGetErrorString(e);
     return -1;
   }
+  ++graph_launches;
+  std::memcpy(T, hT_, n * sizeof(double));
+  std::memcpy(P, hP_, n * sizeof(double));
+  const ReactorStats *st = hstats_;
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, ev0_, ev1_);
+  if (cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) {
+    ms = 0.f;
+    (void)cudaGetLastError();  // timing only: leave no error for the next launch check
+  }
   int nfail = 0;
   for (int r = 0; r < n; ++r) {
     const ReactorStats &q = st[r];
@@ -244,10 +295,11 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     if (cost) cost[r] = q.status == 0 ? q.nsteps : -(double)std::max(1, q.nsteps);
     if (gpu_time) gpu_time[r] = ms * 1e-3 / n;
   }
-  if (stats) *stats = st;
+  if (stats) stats->assign(st, st + n);
   if (tot) {
     *tot = SolveStatsTotals();
-    for (auto &q : st) {
+    for (int r = 0; r < n; ++r) {
+      const ReactorStats &q = st[r];
       tot->nsteps += q.nsteps;
       tot->nrej += q.nrej;
       tot->nnewt += q.nnewt;

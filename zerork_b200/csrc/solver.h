@@ -75,6 +75,16 @@ class ReactorSolver {
   size_t drop_bytes_ = 0;
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  // pinned host staging (fixed addresses for the captured copies)
+  double *hT_ = nullptr, *hP_ = nullptr, *hY_ = nullptr;
+  int *horder_ = nullptr;
+  ReactorStats *hstats_ = nullptr;
+  // one CUDA graph per call configuration: H2D copies, queue reset, the
+  // persistent integration kernel between two timing events, D2H copies
+  cudaGraphExec_t graph_ = nullptr;
+  std::vector<unsigned char> graph_key_;
+ public:
+  long graph_launches = 0, graph_captures = 0;
 };
 
 }  // namespace zrk

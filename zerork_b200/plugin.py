@@ -51,6 +51,9 @@ def plugin_lib():
         L.zerork_reactor_free.argtypes = [vp]
         L.zrk_plugin_last_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_float)]
         L.zrk_plugin_set_predictor.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.zrk_plugin_graph_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        L.zrk_plugin_autotune.argtypes = [vp, C.c_int, C.c_double, vp, vp, vp, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_float)]
         _bound = True
     return L
 
@@ -152,6 +155,24 @@ class Plugin:
         rc = self.L.zrk_plugin_set_predictor(self.h, net.h, *[a.ctypes.data for a in arrs])
         if rc != 0:
             raise PluginError(99, "set_predictor: " + _lib().zrk_last_error().decode())
+
+    def graph_stats(self):
+        c, l = C.c_long(), C.c_long()
+        self.L.zrk_plugin_graph_stats(self.h, C.byref(c), C.byref(l))
+        return {"captures": c.value, "launches": l.value}
+
+    def autotune(self, dt, T, P, Y):
+        """Tune the integrator launch mapping on a sample of these reactors;
+        returns (best setting, kernel ms)."""
+        T = np.ascontiguousarray(T, np.float64)
+        P = np.ascontiguousarray(P, np.float64)
+        Y = np.ascontiguousarray(Y, np.float64)
+        b, ms = C.c_int(), C.c_float()
+        rc = self.L.zrk_plugin_autotune(self.h, T.shape[0], dt, T.ctypes.data, P.ctypes.data,
+                                        Y.ctypes.data, C.byref(b), C.byref(ms))
+        if rc != 0:
+            raise PluginError(99, "autotune: " + _lib().zrk_last_error().decode())
+        return b.value, ms.value
 
     def last_stats(self):
         t = (C.c_long * 7)()
