@@ -47,6 +47,8 @@ def args_():
                         "(profiling captures of one known kernel)")
     p.add_argument("--reactors", type=int, default=2048,
                    help="reactors of the 160-species integration workload (0: skip)")
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the learned-predictor form of the integration leg")
     p.add_argument("--integ-dt", type=float, default=2e-3,
                    help="integration interval per reactor in seconds (2 ms: the workload; "
                         "shorter only for bounded profiling captures)")
@@ -149,7 +151,7 @@ def cpu_reference(files, T, P, Y, budget_s=12.0, nthreads=None):
                       f"({kind} exp) + restated SetupJacobianSparse, {nthreads} OpenMP threads"}
 
 
-def integration_bench(n_reactors, cpu=True, dt=2e-3):
+def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
     """Reactors integrated/s on the 160-species / 900-reaction mechanism (2 ms
     per reactor at rtol 1e-8, atol 1e-20) through the cfd_plugin API with host
     arrays: the plain FP64 path (dense Newton inverse, direct solves) and the
@@ -170,22 +172,25 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3):
         T, P, Y = mechgen.reactor_states(g, n_reactors, "c3", seed=11)
         # learned predictor: pairs from the integrator on other seeded states,
         # trained on the GPU by the library's own kernels
-        from zerork_b200 import predictor as pr
-        t0 = time.perf_counter()
-        T0, P0, Y0 = mechgen.reactor_states(g, 2048, "c3", seed=1001)
-        Xp, Tp = pr.generate_pairs(mf, tf, T0, P0, Y0, rounds=64, seed=5)
-        t_gen = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        net, xs, ts, hist = pr.train(Xp, Tp, epochs=12, batch=1024, lr=1e-3)
-        t_train = time.perf_counter() - t0
-        out["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen, "train_s": t_train,
-                                    "loss_first_last": [hist[0], hist[-1]],
-                                    "network": "163 -> 3 x 256 SiLU -> 161, BF16 weights, FP32 accumulation"}
+        forms = [("plain_fp64", 0, False), ("fp32_krylov", 1, False)]
+        if learned:
+            from zerork_b200 import predictor as pr
+            t0 = time.perf_counter()
+            T0, P0, Y0 = mechgen.reactor_states(g, 2048, "c3", seed=1001)
+            Xp, Tp = pr.generate_pairs(mf, tf, T0, P0, Y0, rounds=64, seed=5)
+            t_gen = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            net, xs, ts, hist = pr.train(Xp, Tp, epochs=12, batch=1024, lr=1e-3)
+            t_train = time.perf_counter() - t0
+            out["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen, "train_s": t_train,
+                                        "loss_first_last": [hist[0], hist[-1]],
+                                        "network": "163 -> 3 x 256 SiLU -> 161, BF16 weights, "
+                                                   "FP32 accumulation"}
+            forms.append(("fp64_learned", 0, True))
         ends = {}
-        for name, fp32, learned in (("plain_fp64", 0, False), ("fp32_krylov", 1, False),
-                                    ("fp64_learned", 0, True)):
+        for name, fp32, use_net in forms:
             p = Plugin(mf, tf, lu_fp32=fp32)
-            if learned:
+            if use_net:
                 p.set_predictor(net, xs, ts)
             cost = p.set_aux_field("COST", np.zeros(n_reactors))
             Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
@@ -207,7 +212,8 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3):
                          "d2h_bytes": int(T.nbytes + P.nbytes + Y.nbytes)}
             p.close()
         out["fp32_over_plain"] = out["fp32_krylov"]["value"] / out["plain_fp64"]["value"]
-        out["learned_over_plain"] = out["fp64_learned"]["value"] / out["plain_fp64"]["value"]
+        if learned:
+            out["learned_over_plain"] = out["fp64_learned"]["value"] / out["plain_fp64"]["value"]
         out["note"] = ("wall time is set by the few reactors that reach max_steps (5000 per attempt, "
                        "5 attempts) and run alone on one SM; which reactors fail differs between forms, "
                        "so ratios between forms at this batch size mostly reflect that tail; compare "
@@ -410,7 +416,8 @@ def main():
         cpu = cpu_reference(files, T, P, Y)
     integ = None
     if rank == 0 and world == 1 and a.reactors > 0:
-        integ = integration_bench(a.reactors, cpu=not a.no_cpu, dt=a.integ_dt)
+        integ = integration_bench(a.reactors, cpu=not a.no_cpu, dt=a.integ_dt,
+                                  learned=not a.no_learned)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "states/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,

@@ -58,6 +58,20 @@ __device__ __forceinline__ double block_sum(double v, double *red) {
   return red[32];
 }
 
+__device__ __forceinline__ double gather4(const double *v, const int *idx, int q0, int q1) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int q = q0;
+  for (; q + 3 < q1; q += 4) {
+    const int i0 = idx[q], i1 = idx[q + 1], i2 = idx[q + 2], i3 = idx[q + 3];
+    a0 += v[i0];
+    a1 += v[i1];
+    a2 += v[i2];
+    a3 += v[i3];
+  }
+  for (; q < q1; ++q) a0 += v[idx[q]];
+  return (a0 + a1) + (a2 + a3);
+}
+
 // ydot at y (shared vector); returns 1 if T <= 0 (all threads agree).
 __device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v,
                        const double *y, double *ydot, bool clamp, double *cv_out) {
@@ -88,9 +102,10 @@ __device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
   __syncthreads();
   double pe = 0.0;
   for (int k = tid; k < S; k += nt) {
-    double des = 0.0, cre = 0.0;
-    for (int q = m.sd_ptr[k]; q < m.sd_ptr[k + 1]; ++q) des += s.ROP[m.sd_step[q]];
-    for (int q = m.sc_ptr[k]; q < m.sc_ptr[k + 1]; ++q) cre += s.ROP[m.sc_step[q]];
+    // four independent partial sums per list keep several rate loads in
+    // flight (the rates of progress may sit in L2)
+    const double des = gather4(s.ROP, m.sd_step, m.sd_ptr[k], m.sd_ptr[k + 1]);
+    const double cre = gather4(s.ROP, m.sc_step, m.sc_ptr[k], m.sc_ptr[k + 1]);
     const double net = cre - des;
     ydot[k] = net * m.mw[k] * v;
     pe += s.U[k] * net * v;
@@ -124,9 +139,8 @@ __device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
     double trow = 0.0;
     for (int kk = k0; kk < k1; ++kk) {
       const int row = m.row_idx[kk];
-      double des = 0.0, cre = 0.0;
-      for (int q = m.nzd_ptr[kk]; q < m.nzd_ptr[kk + 1]; ++q) des += s.ROP[m.nzd_step[q]];
-      for (int q = m.nzc_ptr[kk]; q < m.nzc_ptr[kk + 1]; ++q) cre += s.ROP[m.nzc_step[q]];
+      const double des = gather4(s.ROP, m.nzd_step, m.nzd_ptr[kk], m.nzd_ptr[kk + 1]);
+      const double cre = gather4(s.ROP, m.nzc_step, m.nzc_ptr[kk], m.nzc_ptr[kk + 1]);
       const double val = (0.0 - des * t2) + cre * t2;
       trow += val * s.U[row];
       J[kk] = val * (m.mw[row] * wcol);
