@@ -72,7 +72,8 @@ size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);
 // CTA-per-reactor dense-block integrator (integrator_dense.cu); IntegArgs.state
 // holds the per-reactor Jacobian (state_stride = Jacobian nonzeros).
 // spill: bit 1 puts rates of progress, bit 2 the BDF differences, in a global
-// slice of IntegArgs.rop_scratch per CTA (dense_spill_doubles each).
+// slice of IntegArgs.rop_scratch per CTA (dense_spill_doubles each); bit 4
+// keeps the reactor Jacobian in shared memory instead of IntegArgs.state.
 constexpr int kDenseMaxN = 256;  // dense-block integrator: n = nsp + 1 <= 256
 size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill);
 size_t dense_spill_doubles(const DevMech &m);

@@ -12,6 +12,7 @@ size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill) {
   if (fp32) d += (kMaxl + 3) * (size_t)n;
   if (!(spill & 1)) d += m.nstep;
   if (!(spill & 2)) d += (kMaxOrder + 3) * (size_t)n;
+  if (spill & 4) d += m.nnz;  // reactor Jacobian in shared memory
   size_t bytes = d * sizeof(double) + (size_t)n * lda * (fp32 ? sizeof(float) : sizeof(double));
   return ((bytes + 15) / 16) * 16;
 }

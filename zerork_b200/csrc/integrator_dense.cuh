@@ -39,6 +39,7 @@ struct Smem {
   double *bs;   // n: scaled right-hand side
   double *V;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
   float *mlp;   // learned predictor: two activation buffers of kPredBuf floats
+  double *Jsm;  // reactor Jacobian when it is kept in shared memory (spill bit 4)
 };
 
 // Sum over the CTA; every thread gets thread 0's total (deterministic).
@@ -659,6 +660,9 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
       __syncthreads();
       if (use_pred) predict_cta(m, o, s, v, h);
       const double c = h / bc.alp[q];
+      // new factor when c moved by more than 30 % (CVODE's dgmax); a looser
+      // rule for the FP32 preconditioner costs more Krylov failures than the
+      // factorizations it saves
       if (fabs(c / c_lu - 1.0) > 0.3) {
         st.nlu++;
         c_lu = c;
@@ -828,6 +832,8 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
   s.U = p; p += S;
   if (spill & 1) { s.ROP = g; } else { s.ROP = p; p += N; }
   if (spill & 2) { s.D = g + N; } else { s.D = p; p += (kMaxOrder + 3) * n; }
+  s.Jsm = nullptr;
+  if (spill & 4) { s.Jsm = p; p += m.nnz; }
   s.y = p; p += n;
   s.f = p; p += n;
   s.f0 = p; p += n;
@@ -859,7 +865,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     __syncthreads();
     if (idx >= a.n_reactors) break;
     const int r = a.order ? a.order[idx] : idx;
-    double *J = a.state + (size_t)r * a.state_stride;
+    double *J = (spill & 4) ? s.Jsm : a.state + (size_t)r * a.state_stride;
     const double T0 = a.T[r], P0 = a.P[r];
     const double *Y0 = a.Y + (size_t)r * S;
     double pa = 0.0;

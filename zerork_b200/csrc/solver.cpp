@@ -126,7 +126,10 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   // dense block in shared memory, spilling the rates of progress and then the
   // BDF differences to an L2-resident global slice if needed
   int spill = -1;
-  for (int sp : {0, 1, 3})
+  // preference: the Jacobian beside the factor in shared memory (the FP32
+  // path reads it in every Krylov iteration), then rates of progress and
+  // BDF history spilled to an L2-resident slice
+  for (int sp : {4, 0, 5, 1, 3})
     if (m.nsp + 1 <= kDenseMaxN && dense_smem_bytes(m, o.lu_fp32, nullptr, sp) <= kSmemMax) {
       spill = sp;
       break;
