@@ -174,37 +174,48 @@ __device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
 // species spanning 20 decades of mass fraction and keeps the inverse
 // accurate in the weighted norm the Newton test uses.
 //
-// Gauss-Jordan with partial pivoting, in place.  Row interchanges are
-// accumulated in perm (row i of the factored matrix is row perm[i] of Pw),
-// so A ends as (Pi Pw)^-1 = Pw^-1 Pi^T and the right-hand side is permuted on
-// application instead of unswapping columns.  Two barriers per pivot: phase
-// S picks the pivot from the per-warp candidates (every thread computes the
-// same choice), swaps the rows and scales the pivot row; phase U updates the
-// other rows, warp w owning rows i = w (mod warps), two rows per pass with
-// every load issued before the stores, lane l the columns l (mod 32) with
-// the pivot row in registers, and leaves the candidate for the next column.
-// Returns nonzero (all threads) for a singular or non-finite matrix.
-template <class LT>
-__device__ __forceinline__ void track(double &ca, int &ci, double &cv, LT a, int i) {
-  const double d = fabs((double)a);
+// Gauss-Jordan with partial pivoting, in place, two pivots per sweep of the
+// matrix.  Row interchanges are accumulated in perm (row i of the factored
+// matrix is row perm[i] of Pw), so A ends as (Pi Pw)^-1 = Pw^-1 Pi^T and the
+// right-hand side is permuted on application instead of unswapping columns.
+// Per pair of pivots (k, k+1), four barriers:
+//   S1  pick pivot k from the per-warp candidates (every thread makes the
+//       same choice), swap rows, scaled pivot row r1 (kept in colk);
+//   C   column k+1 as it will be after eliminating column k,
+//       g_i = a_i[k+1] - a_i[k] r1[k+1], gives the candidates for pivot k+1
+//       (each carries its a_i[k]);
+//   S2  pick pivot k+1, swap the raw rows, r2 = scaled (a_{k+1} - a_{k+1}[k]
+//       r1), row k becomes r1 - r1[k+1] r2;
+//   U   every other row in one pass, a_i - a_i[k] r1 - g_i r2 (columns k and
+//       k+1 get their Gauss-Jordan values from the lanes that own them), warp
+//       w owning rows i = w (mod warps), two rows per pass with every load
+//       issued before the stores, lane l the columns l (mod 32) with r1 and
+//       r2 in registers; it leaves the candidates for column k+2.
+// A lone last pivot is swept on its own.  Returns nonzero (all threads) for a
+// singular or non-finite matrix.
+__device__ __forceinline__ void track(double &ca, int &ci, double &cv, double &cf, double a, int i, double f) {
+  const double d = fabs(a);
   if (d > ca) {
     ca = d;
     ci = i;
-    cv = (double)a;
+    cv = a;
+    cf = f;
   }
 }
 
 // Largest |value| over the warp, ties to the lowest row; every lane ends
-// with the same (a, i, v).
-__device__ __forceinline__ void warp_argmax(double &a, int &i, double &v) {
+// with the same (a, i, v, f).
+__device__ __forceinline__ void warp_argmax(double &a, int &i, double &v, double &f) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const double oa = __shfl_xor_sync(kFull, a, o), ov = __shfl_xor_sync(kFull, v, o);
+    const double of = __shfl_xor_sync(kFull, f, o);
     const int oi = __shfl_xor_sync(kFull, i, o);
     if (oa > a || (oa == a && oi < i)) {
       a = oa;
       i = oi;
       v = ov;
+      f = of;
     }
   }
 }
@@ -212,8 +223,9 @@ __device__ __forceinline__ void warp_argmax(double &a, int &i, double &v) {
 template <class LT, int NC>
 __device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda) {
   LT *A = (LT *)s.A;
+  LT *r1b = (LT *)s.colk;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
-  double *cand = s.red + 64;  // [0, 16): |pivot|, [16, 32): row, [32, 48): value
+  double *cand = s.red + 64;  // [0,16) |pivot|, [16,32) row, [32,48) value, [48,64) a_row[k]
   for (int i = tid; i < n * lda; i += nt) A[i] = (LT)0;
   for (int i = tid; i < n; i += nt) {
     s.wlu[i] = s.scale[i];
@@ -230,61 +242,120 @@ __device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, doub
   __syncthreads();
   for (int i = tid; i < n; i += nt) A[i * lda + i] += (LT)1;
   __syncthreads();
-  {  // candidates for column 0
-    double ca = -1.0, cv = 0.0;
-    int ci = n;
-    for (int i = tid; i < n; i += nt) track(ca, ci, cv, A[i * lda], i);
-    warp_argmax(ca, ci, cv);
+  auto publish = [&](double ca, int ci, double cv, double cf) {
+    warp_argmax(ca, ci, cv, cf);
     if (lane == 0) {
       cand[w] = ca;
       cand[16 + w] = (double)ci;
       cand[32 + w] = cv;
+      cand[48 + w] = cf;
     }
+  };
+  // the pivot every thread picks from the candidates; -1 if singular
+  auto pick = [&](double &pv, double &pf) -> int {
+    double best = lane < nw ? cand[lane] : -1.0, v = lane < nw ? cand[32 + lane] : 0.0;
+    double f = lane < nw ? cand[48 + lane] : 0.0;
+    int p = lane < nw ? (int)cand[16 + lane] : n;
+    warp_argmax(best, p, v, f);
+    pv = v;
+    pf = f;
+    return (!(best > 0.0) || !isfinite(best) || p >= n) ? -1 : p;
+  };
+  {  // candidates for column 0
+    double ca = -1.0, cv = 0.0, cf = 0.0;
+    int ci = n;
+    for (int i = tid; i < n; i += nt) track(ca, ci, cv, cf, (double)A[i * lda], i, 0.0);
+    publish(ca, ci, cv, cf);
   }
   __syncthreads();
   int bad = 0;
-  for (int k = 0; k < n; ++k) {
-    // ---- phase S: pivot (warp argmax over the warp candidates, the same in
-    // every warp), row interchange, scaled pivot row
-    double best = lane < nw ? cand[lane] : -1.0, pv = lane < nw ? cand[32 + lane] : 0.0;
-    int p = lane < nw ? (int)cand[16 + lane] : n;
-    warp_argmax(best, p, pv);
-    if (!(best > 0.0) || !isfinite(best) || p >= n) {
+  for (int k = 0; k < n;) {
+    // ---- S1: first pivot of the pair
+    double pv1, unused;
+    const int p1 = pick(pv1, unused);
+    if (p1 < 0) {
       bad = 1;
       break;  // uniform: every thread made the same choice
     }
-    const LT pinv = (LT)1 / (LT)pv;
+    const LT pinv1 = (LT)1 / (LT)pv1;
     if (tid == 0) {
       const int t = s.perm[k];
-      s.perm[k] = s.perm[p];
-      s.perm[p] = t;
+      s.perm[k] = s.perm[p1];
+      s.perm[p1] = t;
     }
     for (int j = tid; j < n; j += nt) {
-      const LT a = A[k * lda + j], b = A[p * lda + j];
-      A[p * lda + j] = a;
-      A[k * lda + j] = (j == k ? (LT)1 : b) * pinv;
+      const LT a = A[k * lda + j], b = A[p1 * lda + j];
+      A[p1 * lda + j] = a;
+      const LT r = (j == k ? (LT)1 : b) * pinv1;
+      A[k * lda + j] = r;
+      r1b[j] = r;
     }
     __syncthreads();
-    // ---- phase U: eliminate column k from every other row.  The register
-    // copy of the pivot row holds 0 in column k, so the uniform update
-    // leaves that entry as it is, and the lane owning column k then stores
-    // its Gauss-Jordan value -f pinv (program order: no race).
-    LT akv[NC];
-    const int ck = k & 31;
+    if (k + 1 == n) {  // lone last pivot
+      for (int i = w; i < n; i += nw) {
+        if (i == k) continue;
+        const LT f = A[i * lda + k];
+        __syncwarp();
+        if (f != (LT)0)
+          for (int j = lane; j < n; j += 32) A[i * lda + j] = (j == k ? (LT)0 : A[i * lda + j]) - f * r1b[j];
+      }
+      __syncthreads();
+      break;
+    }
+    // ---- C: candidates for the second pivot
+    const LT r1k1 = r1b[k + 1];
+    {
+      double ca = -1.0, cv = 0.0, cf = 0.0;
+      int ci = n;
+      for (int i = k + 1 + tid; i < n; i += nt) {
+        const LT f = A[i * lda + k];
+        track(ca, ci, cv, cf, (double)(A[i * lda + k + 1] - f * r1k1), i, (double)f);
+      }
+      publish(ca, ci, cv, cf);
+    }
+    __syncthreads();
+    // ---- S2: second pivot, from the raw row
+    double pv2, f2d;
+    const int p2 = pick(pv2, f2d);
+    if (p2 < 0) {
+      bad = 1;
+      break;
+    }
+    const LT pinv2 = (LT)1 / (LT)pv2, f2 = (LT)f2d;
+    if (tid == 0) {
+      const int t = s.perm[k + 1];
+      s.perm[k + 1] = s.perm[p2];
+      s.perm[p2] = t;
+    }
+    for (int j = tid; j < n; j += nt) {
+      const LT a = A[(k + 1) * lda + j], b = A[p2 * lda + j];
+      A[p2 * lda + j] = a;
+      const LT ap = (j == k ? (LT)0 : b) - f2 * r1b[j];
+      const LT r2 = (j == k + 1 ? (LT)1 : ap) * pinv2;
+      A[(k + 1) * lda + j] = r2;
+      A[k * lda + j] = (j == k + 1 ? (LT)0 : r1b[j]) - r1k1 * r2;
+    }
+    __syncthreads();
+    // ---- U: every other row in one pass
+    LT r1v[NC], r2v[NC];
 #pragma unroll
     for (int t = 0; t < NC; ++t) {
       const int j = lane + 32 * t;
-      akv[t] = (t < NC - 1 || j < n) ? A[k * lda + j] : (LT)0;
-      if (t == (k >> 5) && lane == ck) akv[t] = (LT)0;
+      const bool jv = t < NC - 1 || j < n;
+      r1v[t] = (jv && j != k + 1) ? r1b[j] : (LT)0;
+      r2v[t] = jv ? A[(k + 1) * lda + j] : (LT)0;
     }
-    const int t1 = (k + 1) >> 5, c1 = (k + 1) & 31;
-    double ca = -1.0, cv = 0.0;
+    const LT r1kk = r1b[k], r2k = A[(k + 1) * lda + k], r2k1 = A[(k + 1) * lda + k + 1];
+    const int ck = k & 31, ck1 = (k + 1) & 31, t2 = (k + 2) >> 5, c2 = (k + 2) & 31;
+    double ca = -1.0, cv = 0.0, cf = 0.0;
     int ci = n;
     for (int i0 = w; i0 < n; i0 += 2 * nw) {
       const int i1 = i0 + nw;
       const bool in1 = i1 < n;
-      const LT f0 = (i0 != k) ? A[i0 * lda + k] : (LT)0;  // broadcast reads
-      const LT f1 = (in1 && i1 != k) ? A[i1 * lda + k] : (LT)0;
+      const bool u0 = i0 != k && i0 != k + 1, u1 = in1 && i1 != k && i1 != k + 1;
+      const LT f0 = u0 ? A[i0 * lda + k] : (LT)0, f1 = u1 ? A[i1 * lda + k] : (LT)0;
+      const LT g0 = u0 ? A[i0 * lda + k + 1] - f0 * r1k1 : (LT)0;
+      const LT g1 = u1 ? A[i1 * lda + k + 1] - f1 * r1k1 : (LT)0;
       LT a0[NC], a1[NC];
 #pragma unroll
       for (int t = 0; t < NC; ++t) {
@@ -294,38 +365,39 @@ __device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, doub
         a1[t] = (jv && in1) ? A[i1 * lda + j] : (LT)0;
       }
       __syncwarp();
+      const bool s0 = f0 != (LT)0 || g0 != (LT)0, s1 = f1 != (LT)0 || g1 != (LT)0;
 #pragma unroll
       for (int t = 0; t < NC; ++t) {
         const int j = lane + 32 * t;
         const bool jv = t < NC - 1 || j < n;
-        a0[t] -= f0 * akv[t];
-        a1[t] -= f1 * akv[t];
-        if (jv && f0 != (LT)0) A[i0 * lda + j] = a0[t];
-        if (jv && f1 != (LT)0) A[i1 * lda + j] = a1[t];
+        a0[t] = a0[t] - f0 * r1v[t] - g0 * r2v[t];
+        a1[t] = a1[t] - f1 * r1v[t] - g1 * r2v[t];
+        if (jv && s0) A[i0 * lda + j] = a0[t];
+        if (jv && s1) A[i1 * lda + j] = a1[t];
       }
-      if (lane == ck) {
-        if (f0 != (LT)0) A[i0 * lda + k] = -f0 * pinv;
-        if (f1 != (LT)0) A[i1 * lda + k] = -f1 * pinv;
+      if (lane == ck) {  // Gauss-Jordan values of the eliminated columns
+        if (s0) A[i0 * lda + k] = -f0 * r1kk - g0 * r2k;
+        if (s1) A[i1 * lda + k] = -f1 * r1kk - g1 * r2k;
       }
-      if (lane == c1 && k + 1 < n) {  // candidates for column k + 1
+      if (lane == ck1) {
+        if (s0) A[i0 * lda + k + 1] = -g0 * r2k1;
+        if (s1) A[i1 * lda + k + 1] = -g1 * r2k1;
+      }
+      if (lane == c2 && k + 2 < n) {  // candidates for column k + 2
         LT v0 = a0[0], v1 = a1[0];
 #pragma unroll
         for (int t = 1; t < NC; ++t)
-          if (t == t1) {
+          if (t == t2) {
             v0 = a0[t];
             v1 = a1[t];
           }
-        if (i0 > k) track(ca, ci, cv, v0, i0);
-        if (in1 && i1 > k) track(ca, ci, cv, v1, i1);
+        if (i0 >= k + 2) track(ca, ci, cv, cf, (double)v0, i0, 0.0);
+        if (in1 && i1 >= k + 2) track(ca, ci, cv, cf, (double)v1, i1, 0.0);
       }
     }
-    warp_argmax(ca, ci, cv);
-    if (lane == 0) {
-      cand[w] = ca;
-      cand[16 + w] = (double)ci;
-      cand[32 + w] = cv;
-    }
+    publish(ca, ci, cv, cf);
     __syncthreads();
+    k += 2;
   }
   return __syncthreads_or(bad);
 }
