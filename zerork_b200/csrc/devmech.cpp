@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -126,6 +127,31 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
     jr_ptr.push_back((int)jr_kk.size());
   }
 
+  // cost-sorted work lists (stable: ties keep index order)
+  auto sorted_by = [](std::vector<double> cost) {
+    std::vector<int> idx(cost.size());
+    for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    return idx;
+  };
+  std::vector<double> rc(t.nrxn), sc2(ns), cc(ns);
+  for (int j = 0; j < t.nrxn; ++j) {
+    const RxnRec &R = rec[j];
+    double c = 1.0 + 0.1 * (R.nr + R.np);
+    if (R.flags & (kRevKeq | kRevArr)) c += 1.0;
+    if (R.flags & kThirdBody) c += 0.5 + 0.1 * (t.tb_ptr[R.aux + 1] - t.tb_ptr[R.aux]);
+    if (R.flags & kFalloff) c += 3.0 + 0.1 * (t.fo_ptr[R.aux + 1] - t.fo_ptr[R.aux]);
+    rc[j] = c;
+  }
+  for (int k = 0; k < ns; ++k) {
+    sc2[k] = (sd_ptr[k + 1] - sd_ptr[k]) + (sc_ptr[k + 1] - sc_ptr[k]);
+    double w = 0.0;
+    for (int kk = p.col_ptr[k]; kk < p.col_ptr[k + 1]; ++kk)
+      w += 1.0 + (nzd_ptr[kk + 1] - nzd_ptr[kk]) + (nzc_ptr[kk + 1] - nzc_ptr[kk]);
+    cc[k] = w;
+  }
+  const std::vector<int> rxn_order = sorted_by(rc), spc_order = sorted_by(sc2), col_order = sorted_by(cc);
+
   Blob b;
   size_t o_mw = b.add(t.mw), o_imw = b.add(inv_mw), o_rimw = b.add(ru_inv_mw), o_th = b.add(t.thermo);
   size_t o_rec = b.add(rec);
@@ -136,6 +162,7 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   size_t o_cp = b.add(p.col_ptr), o_ri = b.add(p.row_idx), o_lr = b.add(p.last_row);
   size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
   size_t o_jrp = b.add(jr_ptr), o_jrk = b.add(jr_kk), o_jrc = b.add(jr_col);
+  size_t o_ro = b.add(rxn_order), o_so = b.add(spc_order), o_co = b.add(col_order);
   bytes_ = b.bytes.size();
   check(cudaMalloc(&blob_, bytes_), "cudaMalloc(mechanism tables)");
   check(cudaMemcpy(blob_, b.bytes.data(), bytes_, cudaMemcpyHostToDevice), "cudaMemcpy(mechanism tables)");
@@ -172,6 +199,9 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   view_.jr_ptr = (const int *)P(o_jrp);
   view_.jr_kk = (const int *)P(o_jrk);
   view_.jr_col = (const int *)P(o_jrc);
+  view_.rxn_order = (const int *)P(o_ro);
+  view_.spc_order = (const int *)P(o_so);
+  view_.col_order = (const int *)P(o_co);
 }
 
 DeviceMechanism::~DeviceMechanism() {

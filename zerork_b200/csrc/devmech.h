@@ -54,6 +54,10 @@ struct DevMech {
   // into the compressed-column values) in columns jr_col[p], p in
   // [jr_ptr[i], jr_ptr[i+1])
   const int *jr_ptr, *jr_kk, *jr_col;
+  // work lists sorted by decreasing estimated cost, for snake-order
+  // assignment to thread groups: reactions, species (production gathers),
+  // species Jacobian columns
+  const int *rxn_order, *spc_order, *col_order;
 };
 
 // Host-side builder; owns the device allocation.

@@ -98,8 +98,13 @@ __device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
   }
   const double Csum = block_sum(pc, s.red);
   const double cv = block_sum(pcv, s.red);
-  for (int r = tid; r < m.nrxn; r += nt)
-    reaction_item<1, 1>(m, m.rxn[r], 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum, o.lim);
+  // reactions by decreasing cost in snake order over the threads
+  for (int rr = 0; rr * nt < m.nrxn; ++rr) {
+    const int pos = rr * nt + ((rr & 1) ? nt - 1 - tid : tid);
+    if (pos < m.nrxn)
+      reaction_item<1, 1>(m, m.rxn[m.rxn_order[pos]], 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum,
+                          o.lim);
+  }
   __syncthreads();
   double pe = 0.0;
   for (int k = tid; k < S; k += nt) {
@@ -133,7 +138,8 @@ __device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
   const double multFact = -1.0 / cvc;
   double T = yS * o.Tref;
   if (T > 1.0e4) T = 1.0e4;
-  for (int j = tid; j < S; j += nt) {  // one column per thread
+  for (int jj = tid; jj < S; jj += nt) {  // one column per thread, costliest first
+    const int j = m.col_order[jj];
     const double t2 = m.mw[j] / clamp_mass_fraction(y[j], o.mmf) * v;
     const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
     const double wcol = m.inv_mw[j];

@@ -99,6 +99,13 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
 #define SC(r, k) sc[(r) * TS + q + (k) * GS]
 #define PT(a, ww, k) sPart[((a) * NW + (ww)) * TS + q + (k) * GS]
 #define FORV _Pragma("unroll") for (int k = 0; k < V; ++k)
+// Items of a cost-sorted work list in snake order: round r gives group g the
+// item at r*NG + g (r even) or r*NG + NG-1-g (r odd), so the costliest items
+// spread over the groups and every group's total is close to the mean.
+#define SNAKE(var, list, count)                                      \
+  for (int snake_r = 0, var = 0; snake_r * NG < (count); ++snake_r)  \
+    if (const int snake_p = snake_r * NG + ((snake_r & 1) ? NG - 1 - g : g); \
+        snake_p < (count) && ((var = (list)[snake_p]), true))
   const int ntiles = (n + TS - 1) / TS;
   const double dummy_y = 1.0 / S;
 
@@ -198,14 +205,14 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     __syncthreads();
     FORV Csum[k] = SC(S_CSUM, k);
     // ---- reactions at T
-    for (int r = g; r < m.nrxn; r += NG)
+    SNAKE(r, m.rxn_order, m.nrxn)
       reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
     __syncthreads();
     // ---- net production rates, energy partial
     {
       double pe[V];
       FORV pe[k] = 0.0;
-      for (int s = g; s < S; s += NG) {
+      SNAKE(s, m.spc_order, S) {
         double des[V], cre[V];
         FORV des[k] = cre[k] = 0.0;
         gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
@@ -277,14 +284,14 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       {
         double Cc[V];
         FORV Cc[k] = SC(S_CSUM, k);
-        for (int r = g; r < m.nrxn; r += NG)
+        SNAKE(r, m.rxn_order, m.nrxn)
           reaction_item<TS, V>(m, m.rxn[r], q, sX, sG, sROP, Tr, logT, invT, lprt, Cc, kp.lim);
       }
       __syncthreads();
       {
         double pe[V];
         FORV pe[k] = 0.0;
-        for (int s = g; s < S; s += NG) {
+        SNAKE(s, m.spc_order, S) {
           double des[V], cre[V];
           FORV des[k] = cre[k] = 0.0;
           gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
@@ -312,7 +319,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         TdC[k] = SC(S_TDOTC, k);
         multFact[k] = -1.0 / SC(S_CVC, k);
       }
-      for (int j = g; j < S; j += NG) {
+      SNAKE(j, m.col_order, S) {
         const double mwj = m.mw[j], wcol = m.inv_mw[j];
         const double *th = m.thermo + 16 * j;
         const double riw = m.ru_inv_mw[j];
@@ -395,13 +402,13 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       }
     }
     __syncthreads();
-    for (int r = g; r < m.nrxn; r += NG)
+    SNAKE(r, m.rxn_order, m.nrxn)
       reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
     __syncthreads();
     {
       double pe[V];
       FORV pe[k] = 0.0;
-      for (int s = g; s < S; s += NG) {
+      SNAKE(s, m.spc_order, S) {
         double des[V], cre[V];
         FORV des[k] = cre[k] = 0.0;
         gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
@@ -453,6 +460,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
 #undef SC
 #undef PT
 #undef FORV
+#undef SNAKE
 }
 
 template <int TS, int V, int MAXT>
