@@ -34,11 +34,6 @@ namespace {
 constexpr double kRu = kRuD;
 constexpr double kPatm = kPatmD;
 
-enum Scal {
-  S_T, S_P, S_YS, S_V, S_TR, S_LOGT, S_INVT, S_LPRT, S_CSUM, S_CV, S_TDOT, S_CVC, S_TDOTC,
-  S_YSP, S_MULT, S_CVP, S_TDOTP, kNScal
-};
-
 struct Layout {
   int rC, rU, rX, rG, rROP, rPart, rScal, rows;
 };
@@ -52,8 +47,8 @@ __host__ __device__ inline Layout make_layout(int S, int N, int NG) {
   L.rG = 3 * S;
   L.rROP = 4 * S;
   L.rPart = 4 * S + N;
-  L.rScal = L.rPart + 2 * NG;
-  L.rows = L.rScal + kNScal;
+  L.rScal = L.rPart + 4 * NG;  // two buffers of two partial rows per warp
+  L.rows = L.rScal;
   return L;
 }
 
@@ -95,8 +90,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
   const Layout L = make_layout(S, N, NW);
   double *ws = gscratch ? gscratch + (size_t)blockIdx.x * ws_doubles : smem_dyn;
   double *sC = ws + L.rC * TS, *sU = ws + L.rU * TS, *sX = ws + L.rX * TS, *sG = ws + L.rG * TS;
-  double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS, *sc = ws + L.rScal * TS;
-#define SC(r, k) sc[(r) * TS + q + (k) * GS]
+  double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS;
 #define PT(a, ww, k) sPart[((a) * NW + (ww)) * TS + q + (k) * GS]
 #define FORV _Pragma("unroll") for (int k = 0; k < V; ++k)
 // Items of a cost-sorted work list in snake order: round r gives group g the
@@ -128,36 +122,28 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         FORV pa[k] += yload(s, k) * iw;
       }
       FORV pa[k] = warp_group_sum<GS>(pa[k]);
-      if (wlead) FORV PT(0, w, k) = pa[k];
+      if (wlead) FORV PT(2, w, k) = pa[k];  // second buffer: the species pass follows
     }
     __syncthreads();
-    if (g == 0) {
-      FORV {
-        double sum = 0.0;
-        for (int ww = 0; ww < NW; ++ww) sum += PT(0, ww, k);
-        const double T = valid[k] ? Tin[st[k]] : 1000.0;
-        const double P = valid[k] ? Pin[st[k]] : kPatm;
-        const double yS = T / kp.Tref;
-        const double mwmix = 1.0 / sum;
-        const double rho = P * mwmix / (kRu * T);
-        SC(S_YS, k) = yS;
-        SC(S_V, k) = 1.0 / rho;
-        double Tr = yS * kp.Tref;
-        if (Tr > 1.0e4) Tr = 1.0e4;
-        SC(S_TR, k) = Tr;
-        SC(S_LOGT, k) = log(Tr);
-        SC(S_INVT, k) = 1.0 / Tr;
-        SC(S_LPRT, k) = log(kPatm / (kRu * Tr));
-      }
-    }
-    __syncthreads();
-    double v[V], Tr[V], logT[V], invT[V], lprt[V], Csum[V];
+    // every thread reduces the warp partials of its own states (same order
+    // everywhere, so the values agree) instead of a barrier-fenced one-group
+    // phase
+    double v[V], Tr[V], logT[V], invT[V], lprt[V], Csum[V], yS[V], cv[V], cvc[V];
     FORV {
-      v[k] = SC(S_V, k);
-      Tr[k] = SC(S_TR, k);
-      logT[k] = SC(S_LOGT, k);
-      invT[k] = SC(S_INVT, k);
-      lprt[k] = SC(S_LPRT, k);
+      double sum = 0.0;
+      for (int ww = 0; ww < NW; ++ww) sum += PT(2, ww, k);
+      const double T = valid[k] ? Tin[st[k]] : 1000.0;
+      const double P = valid[k] ? Pin[st[k]] : kPatm;
+      yS[k] = T / kp.Tref;
+      const double mwmix = 1.0 / sum;
+      const double rho = P * mwmix / (kRu * T);
+      v[k] = 1.0 / rho;
+      double t = yS[k] * kp.Tref;
+      if (t > 1.0e4) t = 1.0e4;
+      Tr[k] = t;
+      logT[k] = log(t);
+      invT[k] = 1.0 / t;
+      lprt[k] = log(kPatm / (kRu * t));
     }
     // ---- species pass at T: C, g/RT, u/RT, partial sums
     int need = 0;
@@ -190,20 +176,16 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       }
     }
     need = __syncthreads_or(need);
-    if (g == 0) {
-      FORV {
-        double cs = 0.0, cv = 0.0;
-        for (int ww = 0; ww < NW; ++ww) {
-          cs += PT(0, ww, k);
-          cv += PT(1, ww, k);
-        }
-        SC(S_CSUM, k) = cs;
-        SC(S_CV, k) = cv;
-        SC(S_CVC, k) = cv;
+    FORV {
+      double cs = 0.0, c2 = 0.0;
+      for (int ww = 0; ww < NW; ++ww) {
+        cs += PT(0, ww, k);
+        c2 += PT(1, ww, k);
       }
+      Csum[k] = cs;
+      cv[k] = c2;
+      cvc[k] = c2;
     }
-    __syncthreads();
-    FORV Csum[k] = SC(S_CSUM, k);
     // ---- reactions at T
     SNAKE(r, m.rxn_order, m.nrxn)
       reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
@@ -231,18 +213,18 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       if (wlead) FORV PT(0, w, k) = pe[k];
     }
     __syncthreads();
-    if (g == 0) {
-      FORV {
-        double es = 0.0;
-        for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
-        const double Td = -es * kRu * SC(S_YS, k) / SC(S_CV, k) + 0.0;
-        SC(S_TDOT, k) = Td;
-        SC(S_TDOTC, k) = Td;
-        if (valid[k] && ydot) ydot[(size_t)S * ld + st[k]] = Td;
-      }
+    double td[V], tdc[V];
+    FORV {
+      double es = 0.0;
+      for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
+      td[k] = -es * kRu * yS[k] / cv[k] + 0.0;
+      tdc[k] = td[k];
+      if (g == 0 && valid[k] && ydot) ydot[(size_t)S * ld + st[k]] = td[k];
     }
-    __syncthreads();
-    if (jac == nullptr) continue;
+    if (jac == nullptr) {
+      __syncthreads();  // the next tile reuses the workspace
+      continue;
+    }
     // ---- clamped state (reactor_nvector_serial.cpp:629-640), only if needed
     if (need) {
       {
@@ -263,27 +245,23 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           pc[k] = warp_group_sum<GS>(pc[k]);
           pcv[k] = warp_group_sum<GS>(pcv[k]);
         }
-        if (wlead) FORV {
-          PT(0, w, k) = pc[k];
-          PT(1, w, k) = pcv[k];
-        }
-      }
-      __syncthreads();
-      if (g == 0) {
-        FORV {
-          double cs = 0.0, cv = 0.0;
-          for (int ww = 0; ww < NW; ++ww) {
-            cs += PT(0, ww, k);
-            cv += PT(1, ww, k);
-          }
-          SC(S_CSUM, k) = cs;
-          SC(S_CVC, k) = cv;
+        if (wlead) FORV {  // second buffer: the energy partials may still be read
+          PT(2, w, k) = pc[k];
+          PT(3, w, k) = pcv[k];
         }
       }
       __syncthreads();
       {
         double Cc[V];
-        FORV Cc[k] = SC(S_CSUM, k);
+        FORV {
+          double cs = 0.0, c2 = 0.0;
+          for (int ww = 0; ww < NW; ++ww) {
+            cs += PT(2, ww, k);
+            c2 += PT(3, ww, k);
+          }
+          Cc[k] = cs;
+          cvc[k] = c2;
+        }
         SNAKE(r, m.rxn_order, m.nrxn)
           reaction_item<TS, V>(m, m.rxn[r], q, sX, sG, sROP, Tr, logT, invT, lprt, Cc, kp.lim);
       }
@@ -302,22 +280,19 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         if (wlead) FORV PT(0, w, k) = pe[k];
       }
       __syncthreads();
-      if (g == 0) {
-        FORV {
-          double es = 0.0;
-          for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
-          SC(S_TDOTC, k) = -es * kRu * SC(S_YS, k) / SC(S_CVC, k) + 0.0;
-        }
+      FORV {
+        double es = 0.0;
+        for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
+        tdc[k] = -es * kRu * yS[k] / cvc[k] + 0.0;
       }
-      __syncthreads();
     }
     // ---- analytic Jacobian columns + temperature row
     {
       double RuTemp[V], TdC[V], multFact[V];
       FORV {
-        RuTemp[k] = kRu * SC(S_YS, k);
-        TdC[k] = SC(S_TDOTC, k);
-        multFact[k] = -1.0 / SC(S_CVC, k);
+        RuTemp[k] = kRu * yS[k];
+        TdC[k] = tdc[k];
+        multFact[k] = -1.0 / cvc[k];
       }
       SNAKE(j, m.col_order, S) {
         const double mwj = m.mw[j], wcol = m.inv_mw[j];
@@ -354,27 +329,16 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     }
     __syncthreads();
     // ---- temperature-perturbed RHS for the forward-difference column
-    if (g == 0) {
-      FORV {
-        const double yS = SC(S_YS, k);
-        const double ySp = yS + yS * kp.sqrt_ur;
-        const double dT = ySp - yS;
-        SC(S_YSP, k) = ySp;
-        SC(S_MULT, k) = 1.0 / dT;
-        double Tp = ySp * kp.Tref;
-        if (Tp > 1.0e4) Tp = 1.0e4;
-        SC(S_TR, k) = Tp;
-        SC(S_LOGT, k) = log(Tp);
-        SC(S_INVT, k) = 1.0 / Tp;
-        SC(S_LPRT, k) = log(kPatm / (kRu * Tp));
-      }
-    }
-    __syncthreads();
+    double ysp[V], mult[V];
     FORV {
-      Tr[k] = SC(S_TR, k);
-      logT[k] = SC(S_LOGT, k);
-      invT[k] = SC(S_INVT, k);
-      lprt[k] = SC(S_LPRT, k);
+      ysp[k] = yS[k] + yS[k] * kp.sqrt_ur;
+      mult[k] = 1.0 / (ysp[k] - yS[k]);
+      double Tp = ysp[k] * kp.Tref;
+      if (Tp > 1.0e4) Tp = 1.0e4;
+      Tr[k] = Tp;
+      logT[k] = log(Tp);
+      invT[k] = 1.0 / Tp;
+      lprt[k] = log(kPatm / (kRu * Tp));
     }
     {
       double pcv[V];
@@ -394,14 +358,12 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       if (wlead) FORV PT(1, w, k) = pcv[k];
     }
     __syncthreads();
-    if (g == 0) {
-      FORV {
-        double cv = 0.0;
-        for (int ww = 0; ww < NW; ++ww) cv += PT(1, ww, k);
-        SC(S_CVP, k) = cv;
-      }
+    double cvp[V];
+    FORV {
+      double c2 = 0.0;
+      for (int ww = 0; ww < NW; ++ww) c2 += PT(1, ww, k);
+      cvp[k] = c2;
     }
-    __syncthreads();
     SNAKE(r, m.rxn_order, m.nrxn)
       reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
     __syncthreads();
@@ -423,20 +385,12 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       if (wlead) FORV PT(0, w, k) = pe[k];
     }
     __syncthreads();
-    if (g == 0) {
+    {
+      double tdp[V];
       FORV {
         double es = 0.0;
         for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
-        SC(S_TDOTP, k) = -es * kRu * SC(S_YSP, k) / SC(S_CVP, k) + 0.0;
-      }
-    }
-    __syncthreads();
-    {
-      double mult[V], tdp[V], td[V];
-      FORV {
-        mult[k] = SC(S_MULT, k);
-        tdp[k] = SC(S_TDOTP, k);
-        td[k] = SC(S_TDOT, k);
+        tdp[k] = -es * kRu * ysp[k] / cvp[k] + 0.0;
       }
       const int k0 = m.col_ptr[S], k1 = m.col_ptr[S + 1];
       for (int kk = k0 + g; kk < k1; kk += NG) {
@@ -457,7 +411,6 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     }
     __syncthreads();
   }
-#undef SC
 #undef PT
 #undef FORV
 #undef SNAKE
