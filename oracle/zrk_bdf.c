@@ -42,6 +42,7 @@ void zo_bdf_default_opts(zo_bdf_opts *o) {
   o->max_retries = 5;
   o->retry_atol = 0.1;
   o->retry_rtol = 1.0;
+  o->dT_ign = 0.0;
 }
 
 typedef struct {
@@ -59,6 +60,10 @@ typedef struct {
   double c_lu, crate;
   int jac_current;
   zo_bdf_stats st;
+  /* ignition time: target temperature (<= 0: off), the attempt's start time
+   * within the call, the temperature at the last accepted step */
+  double T_target, t_off, T_prev;
+  double *t_ign;
 } bdf_t;
 
 static double rms(const double *x, const double *s, int n) {
@@ -200,6 +205,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
   double t = 0.0;
   int rc = 0, nsteps_att = 0;
   *t_done = 0.0;
+  b->T_prev = y0[n - 1] * o->Tref;
   memcpy(b->y, y0, sizeof(double) * n);
   if (rhs(b, b->y, b->f0)) return -1;
   /* initial step: Hairer-Norsett-Wanner estimate (first order) */
@@ -308,6 +314,14 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
     }
     for (int k = q; k >= 0; --k)
       for (int i = 0; i < n; ++i) b->D[k * n + i] += b->D[(k + 1) * n + i];
+    if (b->t_ign && b->T_target > 0.0) { /* first crossing of T0 + dT_ign */
+      const double Tn = b->D[n - 1] * o->Tref;
+      if (*b->t_ign < 0.0 && Tn >= b->T_target) {
+        const double frac = (Tn > b->T_prev) ? (b->T_target - b->T_prev) / (Tn - b->T_prev) : 1.0;
+        *b->t_ign = b->t_off + (t - h) + frac * h;
+      }
+      b->T_prev = Tn;
+    }
     if (neq < q + 1) continue;
     double em = INFINITY, ep = INFINITY;
     if (q > 1) {
@@ -344,7 +358,7 @@ failed:
 
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
                      const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
-                     zo_bdf_stats *st) {
+                     const double *y_src, double *t_ign, zo_bdf_stats *st) {
   bdf_t b;
   memset(&b, 0, sizeof(b));
   const int ns = t->nsp, n = ns + 1;
@@ -372,6 +386,10 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   b.tmp = w + 10 * n;
   double *y = (double *)calloc(n, sizeof(double));
   zo_reactor_set_density(b.r, *T, *P, Y);
+  b.r->y_src = y_src;
+  b.t_ign = t_ign;
+  if (t_ign) *t_ign = -1.0;
+  b.T_target = o->dT_ign > 0.0 ? *T + o->dT_ign : -1.0;
   for (int j = 0; j < ns; ++j) y[j] = Y[j];
   y[ns] = *T / o->Tref;
   /* retry loop, solver_cvode.cpp:227-246: a failed attempt restarts the
@@ -384,6 +402,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   int rc = 0;
   for (int attempt = 0;; ++attempt) {
     double t_done = 0.0;
+    b.t_off = dt - t_left;
     rc = integrate(&b, y, t_left, rtol, atol, &t_done);
     if (rc == 0 || attempt + 1 >= o->max_retries) break;
     b.st.retries++;
@@ -409,7 +428,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
 
 int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
                            int nthreads, int n, double dt, double *T, double *P, double *Y,
-                           zo_bdf_stats *stats) {
+                           const double *y_src, double *t_ign, zo_bdf_stats *stats) {
   int nfail = 0;
   if (nthreads < 1) nthreads = 1;
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1) reduction(+ : nfail)
@@ -417,7 +436,9 @@ int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo
     zo_kinetics kin;
     zo_kinetics_oracle(t, &kin);
     zo_bdf_stats st;
-    if (zo_reactor_solve(t, p, &kin, o, dt, &T[r], &P[r], &Y[(size_t)r * t->nsp], &st)) ++nfail;
+    if (zo_reactor_solve(t, p, &kin, o, dt, &T[r], &P[r], &Y[(size_t)r * t->nsp],
+                         y_src ? &y_src[(size_t)r * t->nsp] : NULL, t_ign ? &t_ign[r] : NULL, &st))
+      ++nfail;
     if (stats) stats[r] = st;
   }
   return nfail;

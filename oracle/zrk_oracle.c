@@ -316,9 +316,16 @@ int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot) {
   r->kin.c_from_vy(r->kin.ctx, v, y, r->C);
   r->kin.rates_limiter(r->kin.ctx, T, r->C, r->lim, r->net, r->cre, r->des, r->rop);
   double esum = 0.0;
-  for (int j = 0; j < n; ++j) {
-    ydot[j] = (r->net[j] * r->t->mw[j] * v);
-    esum += r->u_RT[j] * r->net[j] * v;
+  if (r->y_src) { /* reactor_constant_volume_cpu.cpp:108-113 */
+    for (int j = 0; j < n; ++j) {
+      ydot[j] = (r->net[j] * r->t->mw[j] * v + r->y_src[j]);
+      esum += r->u_RT[j] * (r->net[j] * v + r->y_src[j] * (1.0 / r->t->mw[j]));
+    }
+  } else {
+    for (int j = 0; j < n; ++j) {
+      ydot[j] = (r->net[j] * r->t->mw[j] * v);
+      esum += r->u_RT[j] * r->net[j] * v;
+    }
   }
   double dT_dt = -esum * ZO_RU * y[n] / r->mean_cv;
   ydot[n] = dT_dt + (0.0 + 0.0 * v) / (r->mean_cv * r->Tref);

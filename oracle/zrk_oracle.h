@@ -105,6 +105,7 @@ typedef struct zo_reactor {
   double *tmp1, *tmp2, *tmp3;
   double *yscale;  /* [nsp+1] rounding scale of the last ydot: sum of |terms| */
   double *fscale;  /* [nsp+1] yscale of the caller's fy (set by the batch driver) */
+  const double *y_src; /* [nsp] mass-fraction source terms (1/s) or NULL (ZERORK_FIELD_Y_SRC) */
 } zo_reactor;
 
 zo_reactor *zo_reactor_new(const zo_tables *t, const zo_kinetics *kin,

@@ -58,7 +58,7 @@ class ZoBdfOpts(C.Structure):
                 ("nlscoef", C.c_double), ("max_steps", C.c_int), ("Tref", C.c_double),
                 ("min_mass_frac", C.c_double), ("step_limiter", C.c_double),
                 ("analytic", C.c_int), ("max_retries", C.c_int), ("retry_atol", C.c_double),
-                ("retry_rtol", C.c_double)]
+                ("retry_rtol", C.c_double), ("dT_ign", C.c_double)]
 
 
 class ZoBdfStats(C.Structure):
@@ -112,7 +112,7 @@ def _bind_common(lib):
         lib.zo_bdf_default_opts.argtypes = [C.POINTER(ZoBdfOpts)]
         lib.zo_reactor_solve_batch.argtypes = [C.POINTER(ZoTables), C.POINTER(ZoJacPattern),
                                                C.POINTER(ZoBdfOpts), C.c_int, C.c_int, C.c_double,
-                                               _dp, _dp, _dp, C.c_void_p]
+                                               _dp, _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p]
         lib.zo_reactor_solve_batch.restype = C.c_int
     return lib
 
@@ -270,9 +270,12 @@ class OracleTables:
         return wdot, jac, ws, js
 
 
-    def solve(self, T, P, Y, dt, nthreads=1, **opts):
+    def solve(self, T, P, Y, dt, nthreads=1, y_src=None, **opts):
         """Oracle BDF integration of constant-volume reactors (reactor-major Y).
-        Returns (T, P, Y, stats-dict-of-arrays); opts override the plugin defaults."""
+        y_src: optional [n, nsp] mass-fraction source terms.  Returns (T, P,
+        Y, stats-dict-of-arrays); stats["t_ign"] holds the ignition times
+        when opts sets dT_ign > 0 (-1 where not reached).  opts override the
+        plugin defaults."""
         o = ZoBdfOpts()
         self.lib.zo_bdf_default_opts(C.byref(o))
         for k, v in opts.items():
@@ -282,9 +285,13 @@ class OracleTables:
         Y = np.array(Y, dtype=np.float64, order="C")
         n = T.shape[0]
         st = (ZoBdfStats * n)()
-        nf = self.lib.zo_reactor_solve_batch(self.ptr, self.pat, C.byref(o), nthreads, n, float(dt),
-                                             T, P, Y, C.cast(st, C.c_void_p))
+        ys = None if y_src is None else np.ascontiguousarray(y_src, dtype=np.float64)
+        tign = np.full(n, -1.0)
+        self.lib.zo_reactor_solve_batch(self.ptr, self.pat, C.byref(o), nthreads, n, float(dt),
+                                        T, P, Y, None if ys is None else ys.ctypes.data,
+                                        tign.ctypes.data, C.cast(st, C.c_void_p))
         stats = {f: np.array([getattr(st[i], f) for i in range(n)]) for f, _ in ZoBdfStats._fields_}
+        stats["t_ign"] = tign
         return T, P, Y, stats
 
 

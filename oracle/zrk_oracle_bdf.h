@@ -36,6 +36,10 @@ typedef struct zo_bdf_opts {
    * (solver_cvode.cpp:216-246) */
   int max_retries;
   double retry_atol, retry_rtol;
+  /* delta_temperature_ignition: > 0 records the first time T reaches
+   * T0 + dT_ign (ReactorNVectorSerial::RootFunction, :774-784), located by
+   * linear interpolation between the accepted steps that bracket it */
+  double dT_ign;
 } zo_bdf_opts;
 
 typedef struct zo_bdf_stats {
@@ -51,13 +55,13 @@ void zo_bdf_default_opts(zo_bdf_opts *o);
  * On return T, P, Y hold the end state. */
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
                      const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
-                     zo_bdf_stats *st);
+                     const double *y_src, double *t_ign, zo_bdf_stats *st);
 
 /* Batch over reactors (reactor-major Y [n][nsp]) with nthreads OpenMP
  * threads, one reactor object per thread; stats may be NULL. */
 int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
                            int nthreads, int n, double dt, double *T, double *P, double *Y,
-                           zo_bdf_stats *stats);
+                           const double *y_src, double *t_ign, zo_bdf_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -97,6 +97,80 @@ def test_c4_subset_end_states(gpu, fp32, mech_dir):
     _check_against_tight(ot, T, P, Y, 5e-4, Tg, Yg)
 
 
+def test_mass_fraction_sources(gpu, mech_dir):
+    """ZERORK_FIELD_Y_SRC: per-reactor mass-fraction sources added to the
+    species equations and to the energy balance
+    (reactor_constant_volume_cpu.cpp:108-113), against the oracle with the
+    same sources."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 12, "c1", seed=11)
+    pm = zb.Mechanism(mf, tf, device=False)
+    ys = np.zeros_like(Y)
+    ys[:, pm.species.index("N2")] = 10.0  # 1 % of mass added per ms as N2
+    p = Plugin(mf, tf)
+    p.set_aux_field("Y_SRC", ys)
+    Tg, Pg, Yg = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert p.solve(1e-3, Tg, Pg, Yg) == 0
+    ot = oracle_tables(pm)
+    nt = os.cpu_count() or 1
+    To, Po, Yo, so = ot.solve(T, P, Y, 1e-3, nthreads=nt, y_src=ys)
+    Tt, Pt, Yt, st = ot.solve(T, P, Y, 1e-3, nthreads=nt, y_src=ys, rtol=1e-12, atol=1e-24,
+                              max_steps=400000)
+    ok = (so["status"] == 0) & (st["status"] == 0)
+    eo_T, eo_Y = np.abs(To - Tt)[ok], np.max(np.abs(Yo - Yt), axis=1)[ok]
+    fT, fY = 10 * np.median(eo_T), 10 * np.median(eo_Y)
+    assert np.all(np.abs(Tg - Tt)[ok] <= 50 * np.maximum(eo_T, fT) + 1e-5 * Tt[ok])
+    assert np.all(np.max(np.abs(Yg - Yt), axis=1)[ok] <= 50 * np.maximum(eo_Y, fY) + 1e-8)
+    # the sources were applied: about 1e-2 of mass added per reactor
+    assert np.allclose(Yg.sum(axis=1), 1.01, atol=1e-6)
+
+
+def test_ignition_time(gpu, mech_dir):
+    """ZERORK_FIELD_IGNITION_TIME with delta_temperature_ignition: the first
+    time T reaches T0 + delta (the root function of
+    reactor_nvector_serial.cpp:774-784), located by linear interpolation
+    between accepted steps, against the oracle and its tight-tolerance run."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 16, "c1", seed=11)
+    p = Plugin(mf, tf, delta_temperature_ignition=400.0)
+    ign = p.set_aux_field("IGNITION_TIME", np.full(16, -7.0))
+    Tg, Pg, Yg = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert p.solve(1e-3, Tg, Pg, Yg) == 0
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    nt = os.cpu_count() or 1
+    _, _, _, so = ot.solve(T, P, Y, 1e-3, nthreads=nt, dT_ign=400.0)
+    _, _, _, st = ot.solve(T, P, Y, 1e-3, nthreads=nt, dT_ign=400.0, rtol=1e-12, atol=1e-24,
+                           max_steps=400000)
+    to, tt = so["t_ign"], st["t_ign"]
+    assert np.array_equal(ign < 0, tt < 0) and np.any(tt > 0)  # the same reactors ignite
+    hit = tt > 0
+    eo = np.abs(to - tt)[hit]
+    eg = np.abs(ign - tt)[hit]
+    assert np.all(eg <= 50 * np.maximum(eo, 10 * np.median(eo)) + 1e-3 * tt[hit]), (eg, eo)
+    assert np.all(ign[~hit] == -1.0)
+
+
+def test_unsupported_sources_refused(gpu, mech_dir):
+    """Non-zero DPDT / E_SRC sources are refused (not silently ignored)."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 4, "c1", seed=2)
+    p = Plugin(mf, tf)
+    p.set_aux_field("DPDT", np.zeros(4))
+    assert p.solve(1e-4, T.copy(), P.copy(), Y.copy()) == 0
+    p.set_aux_field("E_SRC", np.array([0.0, 0.0, 1.0, 0.0]))
+    from zerork_b200.plugin import PluginError
+    with pytest.raises(PluginError):
+        p.solve(1e-4, T.copy(), P.copy(), Y.copy())
+
+
 def test_failure_leaves_state_and_reports(gpu, mech_dir):
     """max_steps too small: FAILED_SOLVE, state unchanged, negative cost
     (zerork_reactor_manager.cpp:1123-1137)."""

@@ -32,6 +32,7 @@ __device__ __forceinline__ double wsum(double v) {
 struct Warp {
   double *C, *G, *U, *ROP;  // species rows and rates of progress
   void *X;                  // LU work / solve vector (n elements of the LU type)
+  const double *ysrc;       // this reactor's mass-fraction sources (global) or null
 };
 
 struct BdfConst {
@@ -84,8 +85,14 @@ __device__ int rhs_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
     for (int k = m.sd_ptr[s]; k < m.sd_ptr[s + 1]; ++k) des += w.ROP[m.sd_step[k]];
     for (int k = m.sc_ptr[s]; k < m.sc_ptr[s + 1]; ++k) cre += w.ROP[m.sc_step[k]];
     const double net = cre - des;
-    ydot[s] = net * m.mw[s] * v;
-    pe += w.U[s] * net * v;
+    if (w.ysrc) {  // reactor_constant_volume_cpu.cpp:108-113
+      const double ys = w.ysrc[s];
+      ydot[s] = net * m.mw[s] * v + ys;
+      pe += w.U[s] * (net * v + ys * m.inv_mw[s]);
+    } else {
+      ydot[s] = net * m.mw[s] * v;
+      pe += w.U[s] * net * v;
+    }
   }
   const double es = wsum(pe);
   if (lane == 0) ydot[S] = -es * kRuD * yS / cv + 0.0;
@@ -390,12 +397,14 @@ __device__ __forceinline__ double wrms_scaled(const double *x, const double *s, 
 template <class LT>
 __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o, const BdfConst &bc,
                            const Warp &w, const Vecs &V, LT *LU, double v, double t_end,
-                           double rtol, double atol, ReactorStats &st, int lane, double &t_done) {
+                           double rtol, double atol, ReactorStats &st, int lane, double &t_done,
+                           double t_off, double T_target, double &t_ign) {
   const int n = m.nsp + 1;
   LT *x = (LT *)w.X;
   double t = 0.0;
   int rc = 0;
   t_done = 0.0;
+  double T_prev = V.y[m.nsp] * o.Tref;  // ignition: temperature at the last accepted step
   // f0 = f(y0); initial step (Hairer-Norsett-Wanner)
   st.nrhs++;
   if (rhs_warp(m, o, w, v, V.y, V.f0, lane, false, nullptr)) return -1;
@@ -555,6 +564,14 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       for (int k = q; k >= 0; --k) V.D[k * n + i] += V.D[(k + 1) * n + i];
     }
     __syncwarp();
+    if (T_target > 0.0) {  // first crossing of T0 + dT_ign, linear between accepted steps
+      const double Tn = V.D[n - 1] * o.Tref;
+      if (t_ign < 0.0 && Tn >= T_target) {
+        const double frac = (Tn > T_prev) ? (T_target - T_prev) / (Tn - T_prev) : 1.0;
+        t_ign = t_off + (t - h) + frac * h;
+      }
+      T_prev = Tn;
+    }
     if (neq < q + 1) continue;
     double em = INFINITY, ep = INFINITY;
     if (q > 1) {
@@ -619,6 +636,7 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     w.ROP = a.rop_scratch + (size_t)slot * N;
   }
   w.X = after;
+  w.ysrc = nullptr;
   BdfConst bc;
   bdf_consts(bc);
   for (;;) {
@@ -655,10 +673,13 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
-    double t_left = a.dt;
+    double t_left = a.dt, t_ign = -1.0;
+    const double T_target = o.dT_ign > 0.0 ? T0 + o.dT_ign : -1.0;
+    w.ysrc = a.ysrc ? a.ysrc + (size_t)r * S : nullptr;
     for (int attempt = 0;; ++attempt) {
       double t_done = 0.0;
-      rc = bdf_attempt<LT>(m, lu, o, bc, w, V, LU, v, t_left, rtol, atol, rs, lane, t_done);
+      rc = bdf_attempt<LT>(m, lu, o, bc, w, V, LU, v, t_left, rtol, atol, rs, lane, t_done, a.dt - t_left,
+                           T_target, t_ign);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
       t_left -= t_done;
       // solver_cvode.cpp:236-246: adjust tolerances and start over from the
@@ -686,6 +707,7 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     if (lane == 0) {
       a.v[r] = v;
       if (a.stats) a.stats[r] = rs;
+      if (a.t_ign) a.t_ign[r] = t_ign;
     }
     __syncwarp();
   }

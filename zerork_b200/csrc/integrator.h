@@ -46,6 +46,7 @@ struct IntegOpts {
   int lu_fp32;  // factor and apply the Newton matrix in FP32
   double eps_lin;  // Krylov tolerance: eps_lin * nlscoef / error constant (WRMS)
   PredDev pred;    // learned predictor (dense integrator only; enabled = 0: off)
+  double dT_ign;   // delta_temperature_ignition: > 0 records when T reaches T0 + dT_ign
 };
 
 // Per-reactor statistics written by the kernel.
@@ -66,6 +67,8 @@ struct IntegArgs {
   long lu_stride;
   ReactorStats *stats;
   double *rop_scratch;      // optional global ROP rows (one per warp slot)
+  const double *ysrc;       // optional mass-fraction sources [n_reactors][nsp] (1/s)
+  double *t_ign;            // optional ignition times [n_reactors] (-1: not reached)
 };
 
 size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);

@@ -40,6 +40,7 @@ struct Smem {
   double *V;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
   float *mlp;   // learned predictor: two activation buffers of kPredBuf floats
   double *Jsm;  // reactor Jacobian when it is kept in shared memory (spill bit 4)
+  const double *ysrc;  // this reactor's mass-fraction sources (global) or null
 };
 
 // Sum over the CTA; every thread gets thread 0's total (deterministic).
@@ -113,8 +114,14 @@ __device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
     const double des = gather4(s.ROP, m.sd_step, m.sd_ptr[k], m.sd_ptr[k + 1]);
     const double cre = gather4(s.ROP, m.sc_step, m.sc_ptr[k], m.sc_ptr[k + 1]);
     const double net = cre - des;
-    ydot[k] = net * m.mw[k] * v;
-    pe += s.U[k] * net * v;
+    if (s.ysrc) {  // reactor_constant_volume_cpu.cpp:108-113
+      const double ys = s.ysrc[k];
+      ydot[k] = net * m.mw[k] * v + ys;
+      pe += s.U[k] * (net * v + ys * m.inv_mw[k]);
+    } else {
+      ydot[k] = net * m.mw[k] * v;
+      pe += s.U[k] * net * v;
+    }
   }
   const double es = block_sum(pe, s.red);
   if (tid == 0) ydot[S] = -es * kRuD * yS / cv + 0.0;
@@ -659,7 +666,8 @@ __device__ void predict_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
 template <class LT, int NC>
 __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
                            double *J, double v, double t_end, double rtol, double atol,
-                           ReactorStats &st, int lda, double &t_done) {
+                           ReactorStats &st, int lda, double &t_done, double t_off, double T_target,
+                           double &t_ign) {
   const int n = m.nsp + 1, tid = threadIdx.x, nt = blockDim.x;
   auto vrms = [&](const double *x, const double *sc) {
     double a = 0.0;
@@ -672,6 +680,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   double t = 0.0;
   int rc = 0;
   t_done = 0.0;
+  double T_prev = s.y[m.nsp] * o.Tref;  // ignition: temperature at the last accepted step
   st.nrhs++;
   if (rhs_cta(m, o, s, v, s.y, s.f0, false, nullptr)) return -1;
   for (int i = tid; i < n; i += nt) s.scale[i] = atol + fabs(s.y[i]) * rtol;
@@ -851,6 +860,14 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
       for (int k = q; k >= 0; --k) s.D[k * n + i] += s.D[(k + 1) * n + i];
     }
     __syncthreads();
+    if (T_target > 0.0) {  // first crossing of T0 + dT_ign, linear between accepted steps
+      const double Tn = s.D[n - 1] * o.Tref;
+      if (t_ign < 0.0 && Tn >= T_target) {
+        const double frac = (Tn > T_prev) ? (T_target - T_prev) / (Tn - T_prev) : 1.0;
+        t_ign = t_off + (t - h) + frac * h;
+      }
+      T_prev = Tn;
+    }
     if (neq < q + 1) continue;
     double em = INFINITY, ep = INFINITY;
     {
@@ -912,6 +929,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
   if (spill & 2) { s.D = g + N; } else { s.D = p; p += (kMaxOrder + 3) * n; }
   s.Jsm = nullptr;
   if (spill & 4) { s.Jsm = p; p += m.nnz; }
+  s.ysrc = nullptr;
   s.y = p; p += n;
   s.f = p; p += n;
   s.f0 = p; p += n;
@@ -959,10 +977,13 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     // retries (solver_cvode.cpp:227-246): restart the method from the last
     // accepted state for the remaining time with adjusted tolerances;
     // max_steps counts per attempt
-    double t_left = a.dt;
+    double t_left = a.dt, t_ign = -1.0;
+    const double T_target = o.dT_ign > 0.0 ? T0 + o.dT_ign : -1.0;
+    s.ysrc = a.ysrc ? a.ysrc + (size_t)r * S : nullptr;
     for (int attempt = 0;; ++attempt) {
       double t_done = 0.0;
-      rc = attempt_cta<LT, NC>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done);
+      rc = attempt_cta<LT, NC>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done, a.dt - t_left,
+                               T_target, t_ign);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
       t_left -= t_done;
       rs.retries++;
@@ -987,6 +1008,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     if (tid == 0) {
       a.v[r] = v;
       if (a.stats) a.stats[r] = rs;
+      if (a.t_ign) a.t_ign[r] = t_ign;
     }
     __syncthreads();
   }

@@ -210,6 +210,7 @@ static zrk::SolveOptions options_of(zerork_handle_impl *h) {
   o.method = I["gpu_method"];
   o.threads = I["gpu_threads"];
   o.pred = h->pred;
+  o.dT_ign = D["delta_temperature_ignition"];
   return o;
 }
 
@@ -247,8 +248,19 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
     ign = h->own_ign.data();
   }
   const int ns = h->solver->nsp();
+  // pressure-rate and energy sources (reactor_constant_volume_cpu.cpp:87-97)
+  // are not built: refuse non-zero values instead of ignoring them
+  for (int f : {ZERORK_FIELD_DPDT, ZERORK_FIELD_E_SRC})
+    if (const double *x = h->aux[f])
+      for (int r = 0; r < n; ++r)
+        if (x[r] != 0.0) {
+          h->last_error = "non-zero DPDT / E_SRC sources are not supported";
+          std::fprintf(stderr, "zerork_b200: %s\n", h->last_error.c_str());
+          return ZERORK_STATUS_UNKNOWN_ERROR;
+        }
   int nfail = h->solver->solve(o, n, dt, T, P, mf, ns, cost, gpu, tdel,
-                               D["solve_temperature_threshold"], nullptr, &h->last);
+                               D["solve_temperature_threshold"], nullptr, &h->last,
+                               h->aux[ZERORK_FIELD_Y_SRC], ign);
   if (nfail < 0) {
     h->last_error = h->solver->last_error;
     std::fprintf(stderr, "zerork_b200: %s\n", h->last_error.c_str());

@@ -51,6 +51,7 @@ ReactorSolver::ReactorSolver(const std::string &mech, const std::string &therm) 
 ReactorSolver::~ReactorSolver() {
   if (graph_) cudaGraphExecDestroy(graph_);
   cudaFreeHost(hT_); cudaFreeHost(hP_); cudaFreeHost(hY_); cudaFreeHost(horder_); cudaFreeHost(hstats_);
+  cudaFreeHost(hsrc_); cudaFreeHost(hign_); cudaFree(dsrc_); cudaFree(dign_);
   cudaFree(lu_blob_);
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_); cudaFree(drop_);
@@ -64,6 +65,8 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_);
   cudaFreeHost(hT_); cudaFreeHost(hP_); cudaFreeHost(hY_); cudaFreeHost(horder_); cudaFreeHost(hstats_);
+  cudaFreeHost(hsrc_); cudaFreeHost(hign_); cudaFree(dsrc_); cudaFree(dign_);
+  hsrc_ = hign_ = dsrc_ = dign_ = nullptr;
   hT_ = hP_ = hY_ = nullptr;
   horder_ = nullptr;
   hstats_ = nullptr;
@@ -95,6 +98,10 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   if ((e = cudaMallocHost(&hY_, cap * S * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMallocHost(&horder_, cap * sizeof(int))) != cudaSuccess) return e;
   if ((e = cudaMallocHost(&hstats_, cap * sizeof(ReactorStats))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hsrc_, cap * S * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hign_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dsrc_, cap * S * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dign_, cap * sizeof(double))) != cudaSuccess) return e;
   cap_ = cap;
   cap_fp32_ = fp32;
   return cudaSuccess;
@@ -103,7 +110,7 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
 int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
                          int stride, double *cost, double *gpu_time, double *temp_delta,
                          double temp_threshold, std::vector<ReactorStats> *stats,
-                         SolveStatsTotals *tot) {
+                         SolveStatsTotals *tot, const double *ysrc, double *t_ign) {
   if (n <= 0) return 0;
   const int S = tables_.nsp;
   cudaError_t e = reserve(n, o.lu_fp32);
@@ -189,6 +196,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.nlscoef = o.nlscoef;
   io.eps_lin = o.eps_lin;
   io.pred = o.pred;
+  io.dT_ign = o.dT_ign;
   if (io.pred.enabled && method != 1) io.pred.enabled = 0;  // dense integrator only
   io.max_steps = o.max_steps;
   io.max_retries = std::max(1, o.max_retries);
@@ -215,8 +223,11 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   a.lu_stride = lud_.nnz;
   a.stats = dstats_;
   a.rop_scratch = drop_;
+  a.ysrc = ysrc ? dsrc_ : nullptr;
+  a.t_ign = (t_ign && o.dT_ign > 0.0) ? dign_ : nullptr;
   cudaStream_t s = stream_;
   std::memcpy(horder_, order.data(), n * sizeof(int));
+  if (ysrc) std::memcpy(hsrc_, ysrc, (size_t)n * S * sizeof(double));
   if (method == 1) {
     a.state = dstate_;
     a.state_stride = m.nnz;
@@ -248,6 +259,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     q(cudaMemcpyAsync(dP_, hP_, n * sizeof(double), cudaMemcpyHostToDevice, s));
     q(cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
     q(cudaMemcpyAsync(dorder_, horder_, n * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (a.ysrc) q(cudaMemcpyAsync(dsrc_, hsrc_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
     q(cudaMemsetAsync(dhead_, 0, sizeof(int), s));
     q(cudaEventRecordWithFlags(ev0_, s, cudaEventRecordExternal));  // a timing node in the graph
     q(method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)
@@ -257,6 +269,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     q(cudaMemcpyAsync(hP_, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     q(cudaMemcpyAsync(hY_, dY_, (size_t)n * S * sizeof(double), cudaMemcpyDeviceToHost, s));
     q(cudaMemcpyAsync(hstats_, dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s));
+    if (a.t_ign) q(cudaMemcpyAsync(hign_, dign_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     cudaGraph_t g = nullptr;
     const cudaError_t ee = cudaStreamEndCapture(s, &g);
     if (ce == cudaSuccess) ce = ee;
@@ -277,6 +290,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   ++graph_launches;
   std::memcpy(T, hT_, n * sizeof(double));
   std::memcpy(P, hP_, n * sizeof(double));
+  if (a.t_ign) std::memcpy(t_ign, hign_, n * sizeof(double));
   const ReactorStats *st = hstats_;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) {

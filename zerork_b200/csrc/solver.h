@@ -32,6 +32,7 @@ struct SolveOptions {
   int method = 0;         // 0 automatic, 1 CTA dense block, 2 warp sparse LU
   int threads = 0;        // CTA size of the dense method (0 = automatic)
   PredDev pred{};         // learned predictor (dense method only)
+  double dT_ign = 0.0;    // delta_temperature_ignition (> 0: record ignition times)
 };
 
 struct SolveStatsTotals {
@@ -51,9 +52,12 @@ class ReactorSolver {
   // Integrate n reactors (host arrays; mf reactor-major with stride >= nsp).
   // cost/gpu_time/temp_delta may be null.  Returns the number of failed
   // reactors (state left unchanged for those), or -1 on a CUDA error.
+  // ysrc: optional mass-fraction sources [n][nsp] (1/s); t_ign: optional
+  // ignition times [n] (written when o.dT_ign > 0, -1 where not reached).
   int solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
             int stride, double *cost, double *gpu_time, double *temp_delta,
-            double temp_threshold, std::vector<ReactorStats> *stats, SolveStatsTotals *tot);
+            double temp_threshold, std::vector<ReactorStats> *stats, SolveStatsTotals *tot,
+            const double *ysrc = nullptr, double *t_ign = nullptr);
   std::string last_error;
 
  private:
@@ -76,7 +80,8 @@ class ReactorSolver {
   cudaStream_t stream_ = nullptr;
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   // pinned host staging (fixed addresses for the captured copies)
-  double *hT_ = nullptr, *hP_ = nullptr, *hY_ = nullptr;
+  double *hT_ = nullptr, *hP_ = nullptr, *hY_ = nullptr, *hsrc_ = nullptr, *hign_ = nullptr;
+  double *dsrc_ = nullptr, *dign_ = nullptr;
   int *horder_ = nullptr;
   ReactorStats *hstats_ = nullptr;
   // one CUDA graph per call configuration: H2D copies, queue reset, the
