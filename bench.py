@@ -206,6 +206,7 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
                          "newton_iters": st["nnewt"], "rejected": st["nrej"],
                          "factorizations": st["nlu"], "jacobians": st["njac"],
                          "newton_per_step": st["nnewt"] / max(1, st["nsteps"]),
+                         "krylov_per_newton": st["nkry"] / max(1, st["nnewt"]),
                          "max_reactor_steps": int(np.max(np.abs(cost))),
                          "mean_reactor_steps": float(np.mean(np.abs(cost))),
                          "h2d_bytes": int(T.nbytes + P.nbytes + Y.nbytes),

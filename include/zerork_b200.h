@@ -136,6 +136,11 @@ int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, co
 struct zerork_handle_impl;
 int zrk_plugin_last_stats(struct zerork_handle_impl *h, long *totals7, float *kernel_ms);
 
+/* Krylov iterations of the last zerork_reactor_solve call (the FP32 path's
+ * preconditioned FP64 GMRES; 0 on the FP64 path).  No counterpart in the
+ * reference beyond CVODE's linear-iteration counter. */
+int zrk_plugin_krylov_iterations(struct zerork_handle_impl *h, long *iterations);
+
 /* Every zerork_reactor_solve call runs as one CUDA graph (copies in, work
  * queue reset, the persistent integration kernel, copies out), captured when
  * the call's configuration (reactor count, launch mapping, options, dt)

@@ -272,7 +272,7 @@ struct Vecs {
   double *K;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
 };
 
-constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
+constexpr int kMaxl = 10;  // Krylov dimension (no restarts)
 
 // Left-preconditioned GMRES for (I - cJ) x = b on one warp, the Newton
 // system of the FP32 path: the operator is applied in FP64 from the stored
@@ -285,7 +285,7 @@ constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
 // when converged, 1 otherwise.
 template <class LT>
 __device__ int gmres_warp(const DevMech &m, const LUDev &lu, const Vecs &V, const LT *LU, LT *x, double c,
-                          double delta, const double *b, double *xo, int lane) {
+                          double delta, const double *b, double *xo, int lane, int &iters) {
   const int n = lu.n;
   double *Kv = V.K, *u = V.K + (kMaxl + 1) * n, *z = u + n;
   precond_warp<LT>(lu, LU, x, V.wsc, b, z, lane);
@@ -358,6 +358,7 @@ __device__ int gmres_warp(const DevMech &m, const LUDev &lu, const Vecs &V, cons
     g[l] = cc * g[l];
     const double rho = fabs(g[l + 1]);
     nl = l + 1;
+    ++iters;
     if (hn > 0.0)
       for (int i = lane; i < n; i += 32) w[i] /= hn;
     __syncwarp();
@@ -493,7 +494,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
           // tolerance eps_lin * nlscoef / error constant (WRMS); every solve
           // must converge (see integrator_dense.cuh)
           const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
-          if (gmres_warp<LT>(m, lu, V, LU, x, c, delta, V.tmp, V.tmp, lane) != 0) break;
+          if (gmres_warp<LT>(m, lu, V, LU, x, c, delta, V.tmp, V.tmp, lane, st.nkry) != 0) break;
           gs = 1.0;
         } else {
           precond_warp<LT>(lu, LU, x, V.wsc, V.tmp, V.tmp, lane);
@@ -670,7 +671,7 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     for (int s = lane; s < S; s += 32) V.y[s] = Y0[s];
     if (lane == 0) V.y[S] = T0 / o.Tref;
     __syncwarp();
-    ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
+    ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
     double t_left = a.dt, t_ign = -1.0;

@@ -52,6 +52,8 @@ struct IntegOpts {
 // Per-reactor statistics written by the kernel.
 struct ReactorStats {
   int nsteps, nrej, nnewt, njac, nlu, nrhs, status, retries;
+  int nkry;  // Krylov iterations (FP32 path)
+  int pad;
 };
 
 struct IntegArgs {

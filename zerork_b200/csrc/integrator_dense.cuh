@@ -25,7 +25,7 @@ constexpr int kNewtonMaxIter = 3;
 constexpr double kMinFactor = 0.2;
 constexpr double kMaxFactor = 10.0;
 constexpr double kEtaKeep = 1.5;
-constexpr int kMaxl = 5;  // Krylov dimension (SPGMR default, no restarts)
+constexpr int kMaxl = 10;  // Krylov dimension (no restarts)
 constexpr int kPredBuf = 256;  // widest predictor layer (padded)
 
 struct Smem {
@@ -504,7 +504,7 @@ __device__ void make_consts(Consts &b) {
 // when the residual was reduced but not below delta, 2 otherwise.
 template <class LT>
 __device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda,
-                         double delta, const double *b, double *x) {
+                         double delta, const double *b, double *x, int &iters) {
   const int tid = threadIdx.x, nt = blockDim.x;
   double *V = s.V, *u = s.V + (kMaxl + 1) * n, *z = u + n;
   apply_inverse<LT>(s, n, lda, b, z);
@@ -577,6 +577,7 @@ __device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, doubl
     g[l] = cc * g[l];
     rho = fabs(g[l + 1]);
     nl = l + 1;
+    ++iters;
     if (hn > 0.0)
       for (int i = tid; i < n; i += nt) w[i] /= hn;
     if (!isfinite(rho)) return 2;
@@ -780,7 +781,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
           // Krylov solve can pass the Newton test with a poor correction,
           // and a failure here costs only a Jacobian update or a step cut.
           const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
-          if (gmres_cta<LT>(m, s, J, c, n, lda, delta, s.tmp, s.yp) != 0) break;
+          if (gmres_cta<LT>(m, s, J, c, n, lda, delta, s.tmp, s.yp, st.nkry) != 0) break;
           gs = 1.0;  // the Krylov solve uses the current c exactly
         } else {
           apply_inverse<LT>(s, n, lda, s.tmp, s.yp);
@@ -971,7 +972,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     for (int k = tid; k < S; k += nt) s.y[k] = Y0[k];
     if (tid == 0) s.y[S] = T0 / o.Tref;
     __syncthreads();
-    ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0};
+    ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
     // retries (solver_cvode.cpp:227-246): restart the method from the last

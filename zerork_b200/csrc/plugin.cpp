@@ -350,6 +350,12 @@ zerork_status_t zerork_reactor_free(zerork_handle h) {
 
 // Totals of the last solve call: steps, rejected steps, Newton iterations,
 // Jacobians, factorizations, right-hand sides, failed reactors; kernel ms.
+int zrk_plugin_krylov_iterations(zerork_handle h, long *iterations) {
+  if (!h) return ZRK_ERR_INVALID_HANDLE;
+  if (iterations) *iterations = h->last.nkry;
+  return ZRK_OK;
+}
+
 int zrk_plugin_graph_stats(zerork_handle h, long *captures, long *launches) {
   if (!h) return ZRK_ERR_INVALID_HANDLE;
   if (captures) *captures = h->solver ? h->solver->graph_captures : 0;

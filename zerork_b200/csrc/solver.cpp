@@ -323,6 +323,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
       tot->njac += q.njac;
       tot->nlu += q.nlu;
       tot->nrhs += q.nrhs;
+      tot->nkry += q.nkry;
     }
     tot->nfailed = nfail;
     tot->kernel_ms = ms;

@@ -36,7 +36,7 @@ struct SolveOptions {
 };
 
 struct SolveStatsTotals {
-  long nsteps = 0, nrej = 0, nnewt = 0, njac = 0, nlu = 0, nrhs = 0;
+  long nsteps = 0, nrej = 0, nnewt = 0, njac = 0, nlu = 0, nrhs = 0, nkry = 0;
   int nfailed = 0;
   float kernel_ms = 0.f;
   int method = 0;

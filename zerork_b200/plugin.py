@@ -52,6 +52,7 @@ def plugin_lib():
         L.zrk_plugin_last_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_float)]
         L.zrk_plugin_set_predictor.argtypes = [vp, vp, vp, vp, vp, vp]
         L.zrk_plugin_graph_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_long)]
+        L.zrk_plugin_krylov_iterations.argtypes = [vp, C.POINTER(C.c_long)]
         L.zrk_plugin_autotune.argtypes = [vp, C.c_int, C.c_double, vp, vp, vp, C.POINTER(C.c_int),
                                           C.POINTER(C.c_float)]
         _bound = True
@@ -181,4 +182,7 @@ class Plugin:
         keys = ("nsteps", "nrej", "nnewt", "njac", "nlu", "nrhs", "nfailed")
         d = {k: int(t[i]) for i, k in enumerate(keys)}
         d["kernel_ms"] = ms.value
+        k = C.c_long()
+        self.L.zrk_plugin_krylov_iterations(self.h, C.byref(k))
+        d["nkry"] = k.value
         return d
