@@ -45,7 +45,7 @@ def args_():
     p.add_argument("--launch", default="",
                    help="ts,v,warps,global_ws: fixed rates-kernel mapping instead of the autotuner "
                         "(profiling captures of one known kernel)")
-    p.add_argument("--reactors", type=int, default=2048,
+    p.add_argument("--reactors", type=int, default=4096,
                    help="reactors of the 160-species integration workload (0: skip)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-predictor form of the integration leg")
