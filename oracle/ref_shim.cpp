@@ -183,6 +183,28 @@ static void rk_c(void *ctx, double v, const double *y, double *c) {
   static_cast<mechanism *>(ctx)->getCfromVY(v, y, c);
 }
 
+static void rk_h(void *ctx, double T, double *h) {
+  static_cast<mechanism *>(ctx)->getEnthalpy_RT(T, h);
+}
+static double rk_cp(void *ctx, double T, const double *y, double *cp) {
+  return static_cast<mechanism *>(ctx)->getMassCpFromTY(T, y, cp);
+}
+static double rk_mass_u(void *ctx, double T, const double *y) {
+  return static_cast<mechanism *>(ctx)->getMassIntEnergyFromTY(T, y);
+}
+static double rk_mass_h(void *ctx, double T, const double *y) {
+  return static_cast<mechanism *>(ctx)->getMassEnthalpyFromTY(T, y);
+}
+static double rk_pres(void *ctx, double T, double v, const double *y) {
+  return static_cast<mechanism *>(ctx)->getPressureFromTVY(T, v, y);
+}
+static double rk_T_from_E(void *ctx, double E, const double *y, double Tg) {
+  return static_cast<mechanism *>(ctx)->getTemperatureFromEY(E, y, Tg);
+}
+static double rk_T_from_H(void *ctx, double H, const double *y, double Tg) {
+  return static_cast<mechanism *>(ctx)->getTemperatureFromHY(H, y, Tg);
+}
+
 void zrkref_kinetics(void *h, zo_kinetics *k) {
   k->ctx = h;
   k->rates_limiter = rk_rates;
@@ -190,6 +212,31 @@ void zrkref_kinetics(void *h, zo_kinetics *k) {
   k->mass_cv = rk_cv;
   k->density_TPY = rk_dens;
   k->c_from_vy = rk_c;
+  k->enthalpy_RT = rk_h;
+  k->mass_cp = rk_cp;
+  k->mass_int_energy = rk_mass_u;
+  k->mass_enthalpy = rk_mass_h;
+  k->pressure_TVY = rk_pres;
+  k->temp_from_EY = rk_T_from_E;
+  k->temp_from_HY = rk_T_from_H;
+}
+
+// Mixture thermodynamics and reactor right-hand sides (zrk_oracle.h test
+// hooks) on the reference library's own mechanism functions.
+void zrkref_mix_thermo(void *h, int n, const double *T, const double *P, const double *Y,
+                       const double *E, const double *H, double *out) {
+  zo_kinetics k;
+  zrkref_kinetics(h, &k);
+  zo_mix_thermo(&k, static_cast<mechanism *>(h)->getNumSpecies(), n, T, P, Y, E, H, out);
+}
+
+int zrkref_reactor_rhs_batch(void *h, const zo_tables *t, int cp, int n, const double *T0,
+                             const double *P0, const double *Y0, const double *dpdt,
+                             const double *e_src, const double *y_src, const double *tm,
+                             const double *y, double *ydot) {
+  zo_kinetics k;
+  zrkref_kinetics(h, &k);
+  return zo_reactor_rhs_batch(t, &k, cp, n, T0, P0, Y0, dpdt, e_src, y_src, tm, y, ydot);
 }
 
 // Rates + plugin Jacobian over many states on the reference library, one

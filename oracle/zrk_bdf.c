@@ -43,6 +43,7 @@ void zo_bdf_default_opts(zo_bdf_opts *o) {
   o->retry_atol = 0.1;
   o->retry_rtol = 1.0;
   o->dT_ign = 0.0;
+  o->constant_volume = 1;
 }
 
 typedef struct {
@@ -75,17 +76,21 @@ static double rms(const double *x, const double *s, int n) {
   return sqrt(a / n);
 }
 
-static int rhs(bdf_t *b, const double *y, double *f) {
+/* f = ydot(t, y), t local to the attempt (the reactor's sources see the
+ * time from the start of the call) */
+static int rhs(bdf_t *b, double t, const double *y, double *f) {
   b->st.nrhs++;
-  if (zo_cv_rhs(b->r, y, f)) return 1;
+  b->r->time = b->t_off + t;
+  if (zo_reactor_rhs(b->r, y, f)) return 1;
   for (int i = 0; i < b->n; ++i)
     if (!isfinite(f[i])) return 1;
   return 0;
 }
 
 /* Jacobian at y with f = f(y), then Newton matrix A = I - c J, LU. */
-static int take_jacobian(bdf_t *b, const double *y, const double *f) {
+static int take_jacobian(bdf_t *b, double t, const double *y, const double *f) {
   b->st.njac++;
+  b->r->time = b->t_off + t;
   if (!b->o->analytic) {
     /* forward differences, increment sqrt(uround) * max(|y_j|, 1/w_j) */
     const int n = b->n;
@@ -95,7 +100,7 @@ static int take_jacobian(bdf_t *b, const double *y, const double *f) {
       double inc = sqrt(2.220446049250313e-16) * fmax(fabs(y[j]), b->o->atol + b->o->rtol * fabs(y[j]) + 1e-10);
       yp[j] = y[j] + inc;
       inc = yp[j] - y[j];
-      if (rhs(b, yp, fp)) return 1;
+      if (rhs(b, t, yp, fp)) return 1;
       for (int i = 0; i < n; ++i) b->Jd[i * n + j] = (fp[i] - f[i]) / inc;
       yp[j] = y[j];
     }
@@ -207,7 +212,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
   *t_done = 0.0;
   b->T_prev = y0[n - 1] * o->Tref;
   memcpy(b->y, y0, sizeof(double) * n);
-  if (rhs(b, b->y, b->f0)) return -1;
+  if (rhs(b, 0.0, b->y, b->f0)) return -1;
   /* initial step: Hairer-Norsett-Wanner estimate (first order) */
   for (int i = 0; i < n; ++i) b->scale[i] = atol + fabs(b->y[i]) * rtol;
   double d0 = rms(b->y, b->scale, n), d1 = rms(b->f0, b->scale, n);
@@ -215,7 +220,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
   if (h0 > t_end) h0 = t_end;
   for (int i = 0; i < n; ++i) b->tmp[i] = b->y[i] + h0 * b->f0[i];
   double d2 = 0.0;
-  if (rhs(b, b->tmp, b->f) == 0) {
+  if (rhs(b, h0, b->tmp, b->f) == 0) {
     for (int i = 0; i < n; ++i) b->dy[i] = b->f[i] - b->f0[i];
     d2 = rms(b->dy, b->scale, n) / h0;
   }
@@ -227,7 +232,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
   memset(b->D, 0, sizeof(double) * (MAXO + 3) * n);
   memcpy(b->D, b->y, sizeof(double) * n);
   for (int i = 0; i < n; ++i) b->D[n + i] = b->f0[i] * h;
-  if (take_jacobian(b, b->y, b->f0)) { rc = -2; goto failed; }
+  if (take_jacobian(b, 0.0, b->y, b->f0)) { rc = -2; goto failed; }
   if (factor(b, h / b->alp[q])) { rc = -3; goto failed; }
   while (t < t_end) {
     if (nsteps_att >= o->max_steps) { rc = -4; goto failed; }
@@ -264,7 +269,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
       double dnorm_old = -1.0;
       const double gscale = (c == b->c_lu) ? 1.0 : 2.0 / (1.0 + c / b->c_lu);
       for (it = 0; it < NEWTON_MAXITER; ++it) {
-        if (rhs(b, b->y, b->f)) break;
+        if (rhs(b, t_new, b->y, b->f)) break;
         if (it == 0) memcpy(b->f0, b->f, sizeof(double) * n);
         b->st.nnewt++;
         for (int i = 0; i < n; ++i) b->dy[i] = c * b->f[i] - b->psi[i] - b->d[i];
@@ -279,8 +284,8 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
       }
       if (!conv) {
         if (!b->jac_current) {
-          if (rhs(b, b->ypred, b->f0)) { rc = -6; goto failed; }
-          if (take_jacobian(b, b->ypred, b->f0)) { rc = -2; goto failed; }
+          if (rhs(b, t_new, b->ypred, b->f0)) { rc = -6; goto failed; }
+          if (take_jacobian(b, t_new, b->ypred, b->f0)) { rc = -2; goto failed; }
           if (factor(b, c)) { rc = -3; goto failed; }
           continue;
         }
@@ -358,7 +363,8 @@ failed:
 
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
                      const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
-                     const double *y_src, double *t_ign, zo_bdf_stats *st) {
+                     const double *y_src, double dpdt, double e_src, double *t_ign,
+                     zo_bdf_stats *st) {
   bdf_t b;
   memset(&b, 0, sizeof(b));
   const int ns = t->nsp, n = ns + 1;
@@ -385,8 +391,8 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   b.d = w + 5 * n; b.dy = w + 6 * n; b.scale = w + 7 * n; b.rhs = w + 8 * n; b.err = w + 9 * n;
   b.tmp = w + 10 * n;
   double *y = (double *)calloc(n, sizeof(double));
-  zo_reactor_set_density(b.r, *T, *P, Y);
-  b.r->y_src = y_src;
+  b.r->cp = o->constant_volume == 0;
+  zo_reactor_init_state(b.r, *T, *P, Y, dpdt, e_src, y_src);
   b.t_ign = t_ign;
   if (t_ign) *t_ign = -1.0;
   b.T_target = o->dT_ign > 0.0 ? *T + o->dT_ign : -1.0;
@@ -416,9 +422,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   if (rc == 0) {
     *T = y[ns] * o->Tref;
     for (int j = 0; j < ns; ++j) Y[j] = y[j];
-    double s = 0.0;
-    for (int j = 0; j < ns; ++j) s += Y[j] * (1.0 / t->mw[j]);
-    *P = ZO_RU * (*T) / (b.r->inv_density * (1.0 / s));
+    *P = zo_reactor_pressure(b.r, dt, *T, Y);
   }
   if (st) *st = b.st;
   free(y); free(w); free(b.piv); free(b.A); free(b.Jd); free(b.jac); free(b.D);
@@ -428,7 +432,8 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
 
 int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
                            int nthreads, int n, double dt, double *T, double *P, double *Y,
-                           const double *y_src, double *t_ign, zo_bdf_stats *stats) {
+                           const double *y_src, const double *dpdt, const double *e_src,
+                           double *t_ign, zo_bdf_stats *stats) {
   int nfail = 0;
   if (nthreads < 1) nthreads = 1;
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1) reduction(+ : nfail)
@@ -437,7 +442,8 @@ int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo
     zo_kinetics_oracle(t, &kin);
     zo_bdf_stats st;
     if (zo_reactor_solve(t, p, &kin, o, dt, &T[r], &P[r], &Y[(size_t)r * t->nsp],
-                         y_src ? &y_src[(size_t)r * t->nsp] : NULL, t_ign ? &t_ign[r] : NULL, &st))
+                         y_src ? &y_src[(size_t)r * t->nsp] : NULL, dpdt ? dpdt[r] : 0.0,
+                         e_src ? e_src[r] : 0.0, t_ign ? &t_ign[r] : NULL, &st))
       ++nfail;
     if (stats) stats[r] = st;
   }

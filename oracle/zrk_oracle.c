@@ -252,6 +252,91 @@ static void ok_c_from_vy(void *ctx, double v, const double *y, double *c) {
   for (int j = 0; j < t->nsp; ++j) c[j] = dens * (1.0 / t->mw[j]) * y[j];
 }
 
+/* mechanism.cpp:366-367 getEnthalpy_RT */
+static void ok_h_RT(void *ctx, double T, double *h) { zo_h_RT((const zo_tables *)ctx, T, h); }
+/* mechanism.cpp:408-420 getMassCpFromTY */
+static double ok_mass_cp(void *ctx, double T, const double *y, double *cp) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double mix = 0.0;
+  zo_cp_R(t, T, cp);
+  for (int j = 0; j < t->nsp; ++j) {
+    cp[j] *= ZO_RU / t->mw[j];
+    mix += cp[j] * y[j];
+  }
+  return mix;
+}
+/* mechanism.cpp:355-367 getMassIntEnergyFromTY */
+static double ok_mass_u(void *ctx, double T, const double *y) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double *u = (double *)zcalloc(t->nsp, sizeof(double)), mix = 0.0;
+  zo_h_RT(t, T, u);
+  for (int j = 0; j < t->nsp; ++j) {
+    u[j] -= 1.0;
+    u[j] *= ZO_RU / t->mw[j] * T;
+    mix += u[j] * y[j];
+  }
+  free(u);
+  return mix;
+}
+/* mechanism.cpp:336-347 getMassEnthalpyFromTY */
+static double ok_mass_h(void *ctx, double T, const double *y) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double *h = (double *)zcalloc(t->nsp, sizeof(double)), mix = 0.0;
+  zo_h_RT(t, T, h);
+  for (int j = 0; j < t->nsp; ++j) {
+    h[j] *= ZO_RU / t->mw[j] * T;
+    mix += h[j] * y[j];
+  }
+  free(h);
+  return mix;
+}
+/* mechanism.cpp:292-297 getPressureFromTVY */
+static double ok_pressure(void *ctx, double T, double v, const double *y) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  double s = 0.0;
+  for (int j = 0; j < t->nsp; ++j) s += y[j] * (1.0 / t->mw[j]);
+  double mwmix = 1.0 / s;
+  return ZO_RU * T / (v * mwmix);
+}
+/* mechanism.cpp:477-547 getTemperatureFromEY / getTemperatureFromHY: Newton
+ * on the mixture energy between 100 K and 5000 K (linear extrapolation
+ * outside), steps clipped to +-100 K, stop below 1e-6 K or when the step no
+ * longer changes T, at most 400 iterations.  Both iterations divide by the
+ * mixture c_v, and so does the extrapolation above 5000 K; only the
+ * enthalpy extrapolation below 100 K uses c_p. */
+static double ok_temp_from(void *ctx, int enthalpy, double E, const double *y, double Tg) {
+  const zo_tables *t = (const zo_tables *)ctx;
+  const double Tmin = 100.0, Tmax = 5000.0;
+  double *tmp = (double *)zcalloc(t->nsp, sizeof(double));
+  double (*energy)(void *, double, const double *) = enthalpy ? ok_mass_h : ok_mass_u;
+  const double Emin = energy(ctx, Tmin, y), Emax = energy(ctx, Tmax, y);
+  double T;
+  if (E < Emin) {
+    const double c = enthalpy ? ok_mass_cp(ctx, Tmin, y, tmp) : ok_mass_cv(ctx, Tmin, y, tmp);
+    T = Tmin - (Emin - E) / c;
+  } else if (E > Emax) {
+    T = Tmax - (Emax - E) / ok_mass_cv(ctx, Tmax, y, tmp);
+  } else {
+    T = Tg;
+    if (T < Tmin || T > Tmax) T = Tmin + (Tmax - Tmin) / (Emax - Emin) * (E - Emin);
+    for (int i = 0; i < 400; ++i) {
+      const double Ei = energy(ctx, T, y);
+      const double c = ok_mass_cv(ctx, T, y, tmp);
+      const double dT = fmin(fmax((E - Ei) / c, -100.0), 100.0);
+      if (fabs(dT) < 1.0e-6 || T + dT == T) break;
+      T += dT;
+    }
+  }
+  free(tmp);
+  return T;
+}
+static double ok_temp_from_E(void *ctx, double E, const double *y, double Tg) {
+  return ok_temp_from(ctx, 0, E, y, Tg);
+}
+static double ok_temp_from_H(void *ctx, double H, const double *y, double Tg) {
+  return ok_temp_from(ctx, 1, H, y, Tg);
+}
+
 void zo_kinetics_oracle(const zo_tables *t, zo_kinetics *k) {
   k->ctx = (void *)t;
   k->rates_limiter = ok_rates;
@@ -259,6 +344,13 @@ void zo_kinetics_oracle(const zo_tables *t, zo_kinetics *k) {
   k->mass_cv = ok_mass_cv;
   k->density_TPY = ok_density;
   k->c_from_vy = ok_c_from_vy;
+  k->enthalpy_RT = ok_h_RT;
+  k->mass_cp = ok_mass_cp;
+  k->mass_int_energy = ok_mass_u;
+  k->mass_enthalpy = ok_mass_h;
+  k->pressure_TVY = ok_pressure;
+  k->temp_from_EY = ok_temp_from_E;
+  k->temp_from_HY = ok_temp_from_H;
 }
 
 /* ------------------------------------------------------------- reactor */
@@ -303,16 +395,54 @@ void zo_reactor_set_density(zo_reactor *r, double T, double P, const double *Y) 
   r->inv_density = 1.0 / r->kin.density_TPY(r->kin.ctx, T, P, Y);
 }
 
-/* reactor_constant_volume_cpu.cpp:64-128 GetTimeDerivative, with no
- * energy/pressure/mass sources (dpdt = e_src = 0, y_src = NULL). */
-int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot) {
+void zo_reactor_init_state(zo_reactor *r, double T, double P, const double *Y, double dpdt,
+                           double e_src, const double *y_src) {
+  r->time = 0.0;
+  r->P0 = P;
+  r->T0 = T;
+  r->inv_density = 1.0 / r->kin.density_TPY(r->kin.ctx, T, P, Y);
+  r->E0 = r->cp ? r->kin.mass_enthalpy(r->kin.ctx, T, Y) : r->kin.mass_int_energy(r->kin.ctx, T, Y);
+  r->dpdt = dpdt;
+  r->e_src = e_src;
+  r->y_src = y_src;
+}
+
+double zo_reactor_pressure(const zo_reactor *r, double t, double T, const double *Y) {
+  if (r->cp && !r->y_src) return r->P0 + r->dpdt * t;
+  const double P = r->kin.pressure_TVY(r->kin.ctx, T, r->inv_density, Y);
+  return r->cp ? P : P + r->dpdt * t;
+}
+
+/* GetTimeDerivative: reactor_constant_volume_cpu.cpp:64-128 (cp = 0) and
+ * reactor_constant_pressure_cpu.cpp:71-135 (cp = 1).  The constant-pressure
+ * reactor updates inv_density from the current pressure unless mass sources
+ * are set, as the reference's member does; the constant-volume reactor
+ * keeps it and uses the pressure-rate corrected density locally. */
+int zo_reactor_rhs(zo_reactor *r, const double *y, double *ydot) {
   const int n = r->nsp;
+  const double dt = r->time;
   double T = y[n] * r->Tref;
   if (T <= 0.0) return 1;
   if (T > 1.0e4) T = 1.0e4;
-  r->kin.int_energy_RT(r->kin.ctx, T, r->u_RT);
-  r->mean_cv = r->kin.mass_cv(r->kin.ctx, T, y, r->cv_spc);
-  const double v = r->inv_density;
+  double v = r->inv_density;
+  if (r->cp) {
+    if (!r->y_src) {
+      const double Pc = r->P0 + r->dpdt * dt;
+      r->inv_density = 1.0 / r->kin.density_TPY(r->kin.ctx, T, Pc, y);
+      v = r->inv_density;
+    }
+    if (r->e_src != 0.0) T = r->kin.temp_from_HY(r->kin.ctx, r->E0 + r->e_src * dt, y, T);
+    r->kin.enthalpy_RT(r->kin.ctx, T, r->u_RT);
+    r->mean_cv = r->kin.mass_cp(r->kin.ctx, T, y, r->cv_spc);
+  } else {
+    if (r->e_src != 0.0) T = r->kin.temp_from_EY(r->kin.ctx, r->E0 + r->e_src * dt, y, T);
+    r->kin.int_energy_RT(r->kin.ctx, T, r->u_RT);
+    r->mean_cv = r->kin.mass_cv(r->kin.ctx, T, y, r->cv_spc);
+    if (r->dpdt != 0.0) {
+      const double Pc = r->kin.pressure_TVY(r->kin.ctx, T, r->inv_density, y) + r->dpdt * dt;
+      v = 1.0 / r->kin.density_TPY(r->kin.ctx, T, Pc, y);
+    }
+  }
   r->kin.c_from_vy(r->kin.ctx, v, y, r->C);
   r->kin.rates_limiter(r->kin.ctx, T, r->C, r->lim, r->net, r->cre, r->des, r->rop);
   double esum = 0.0;
@@ -328,7 +458,7 @@ int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot) {
     }
   }
   double dT_dt = -esum * ZO_RU * y[n] / r->mean_cv;
-  ydot[n] = dT_dt + (0.0 + 0.0 * v) / (r->mean_cv * r->Tref);
+  ydot[n] = dT_dt + (r->e_src + r->dpdt * v) / (r->mean_cv * r->Tref);
   double es = 0.0;
   for (int j = 0; j < n; ++j) {
     double m = fabs(r->cre[j]) + fabs(r->des[j]);
@@ -337,6 +467,41 @@ int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot) {
   }
   r->yscale[n] = es * ZO_RU * fabs(y[n]) / fabs(r->mean_cv);
   return 0;
+}
+
+void zo_mix_thermo(const zo_kinetics *k, int nsp, int n, const double *T, const double *P,
+                   const double *Y, const double *E, const double *H, double *out) {
+  double *tmp = (double *)zcalloc(nsp, sizeof(double));
+  for (int s = 0; s < n; ++s) {
+    const double *y = Y + (size_t)s * nsp;
+    double *o = out + 7 * (size_t)s;
+    o[0] = k->density_TPY(k->ctx, T[s], P[s], y);
+    o[1] = k->pressure_TVY(k->ctx, T[s], 1.0 / o[0], y);
+    o[2] = k->mass_int_energy(k->ctx, T[s], y);
+    o[3] = k->mass_enthalpy(k->ctx, T[s], y);
+    o[4] = k->mass_cp(k->ctx, T[s], y, tmp);
+    o[5] = k->temp_from_EY(k->ctx, E[s], y, T[s]);
+    o[6] = k->temp_from_HY(k->ctx, H[s], y, T[s]);
+  }
+  free(tmp);
+}
+
+int zo_reactor_rhs_batch(const zo_tables *t, const zo_kinetics *k, int cp, int n,
+                         const double *T0, const double *P0, const double *Y0,
+                         const double *dpdt, const double *e_src, const double *y_src,
+                         const double *tm, const double *y, double *ydot) {
+  const int ns = t->nsp;
+  int nfail = 0;
+  zo_reactor *r = zo_reactor_new(t, k, 1.0, 1.0e-30, 1.0e22);
+  r->cp = cp;
+  for (int s = 0; s < n; ++s) {
+    zo_reactor_init_state(r, T0[s], P0[s], Y0 + (size_t)s * ns, dpdt ? dpdt[s] : 0.0,
+                          e_src ? e_src[s] : 0.0, y_src ? y_src + (size_t)s * ns : NULL);
+    r->time = tm[s];
+    if (zo_reactor_rhs(r, y + (size_t)s * (ns + 1), ydot + (size_t)s * (ns + 1))) ++nfail;
+  }
+  zo_reactor_free(r);
+  return nfail;
 }
 
 /* ------------------------------------------------------ Jacobian pattern */
@@ -428,7 +593,7 @@ int zo_jac_values(zo_reactor *r, const zo_jac_pattern *p, const double *y, const
     t2[j] = mw[j] / t1[j] * r->inv_density;
   }
   t1[ns] = y[ns];
-  if (zo_cv_rhs(r, t1, t3)) return 1;
+  if (zo_reactor_rhs(r, t1, t3)) return 1;
   for (int k = 0; k < p->nnz; ++k) jac[k] = 0.0;
   if (scale)
     for (int k = 0; k < p->nnz; ++k) scale[k] = 0.0;
@@ -473,7 +638,7 @@ int zo_jac_values(zo_reactor *r, const zo_jac_pattern *p, const double *y, const
   dT = t1[ns] - y[ns];
   const double mult = 1.0 / dT;
   for (int j = 0; j < ns; ++j) t1[j] = y[j];
-  if (zo_cv_rhs(r, t1, t3)) return 1;
+  if (zo_reactor_rhs(r, t1, t3)) return 1;
   for (int k = p->col_ptr[ns]; k < p->col_ptr[nv]; ++k) {
     int row = p->row_idx[k];
     jac[k] = (t3[row] - fy[row]) * mult;
@@ -517,7 +682,7 @@ int zo_batch_rates_jac(const zo_tables *t, const zo_jac_pattern *p, const zo_kin
       zo_reactor_set_density(r, T[s], P[s], Ys);
       for (int j = 0; j < ns; ++j) y[j] = Ys[j];
       y[ns] = T[s] / Tref;
-      if (zo_cv_rhs(r, y, fy)) { ++nfail; continue; }
+      if (zo_reactor_rhs(r, y, fy)) { ++nfail; continue; }
       if (wdot) memcpy(wdot + s * ns, r->net, sizeof(double) * ns);
       if (ydot) memcpy(ydot + s * nv, fy, sizeof(double) * nv);
       if (jac && zo_jac_values(r, p, y, fy, jac + s * (long)p->nnz, NULL)) ++nfail;
@@ -544,7 +709,7 @@ int zo_batch_rates_jac_scaled(const zo_tables *t, const zo_jac_pattern *p, int n
     zo_reactor_set_density(r, T[s], P[s], Ys);
     for (int j = 0; j < ns; ++j) y[j] = Ys[j];
     y[ns] = T[s] / Tref;
-    if (zo_cv_rhs(r, y, fy)) { ++nfail; continue; }
+    if (zo_reactor_rhs(r, y, fy)) { ++nfail; continue; }
     memcpy(wdot + s * ns, r->net, sizeof(double) * ns);
     for (int j = 0; j < ns; ++j) wscale[s * ns + j] = fabs(r->cre[j]) + fabs(r->des[j]);
     memcpy(r->fscale, r->yscale, sizeof(double) * nv);

@@ -90,17 +90,36 @@ typedef struct zo_kinetics {
   double (*mass_cv)(void *ctx, double T, const double *y, double *cv_spc);
   double (*density_TPY)(void *ctx, double T, double P, const double *y);
   void (*c_from_vy)(void *ctx, double v, const double *y, double *c);
+  /* constant-pressure reactor and energy/pressure sources
+   * (src/zerork/mechanism.cpp:292-547) */
+  void (*enthalpy_RT)(void *ctx, double T, double *h_RT);
+  double (*mass_cp)(void *ctx, double T, const double *y, double *cp_spc);
+  double (*mass_int_energy)(void *ctx, double T, const double *y);
+  double (*mass_enthalpy)(void *ctx, double T, const double *y);
+  double (*pressure_TVY)(void *ctx, double T, double v, const double *y);
+  double (*temp_from_EY)(void *ctx, double E, const double *y, double T_guess);
+  double (*temp_from_HY)(void *ctx, double H, const double *y, double T_guess);
 } zo_kinetics;
 
 void zo_kinetics_oracle(const zo_tables *t, zo_kinetics *k);
 
-/* Constant-volume reactor state (applications/cfd_plugin/
- * reactor_constant_volume_cpu.cpp:15-41 InitializeState). */
+/* Reactor state: constant volume (applications/cfd_plugin/
+ * reactor_constant_volume_cpu.cpp:15-41 InitializeState) or constant
+ * pressure (reactor_constant_pressure_cpu.cpp:15-41).  u_RT, cv_spc and
+ * mean_cv hold the reactor's energy_, cx_mass_ and mean_cx_mass_: internal
+ * energy and c_v for constant volume, enthalpy and c_p for constant
+ * pressure. */
 typedef struct zo_reactor {
   const zo_tables *t;
   zo_kinetics kin;
   int nsp, nstep;
   double inv_density, Tref, min_mass_frac;
+  int cp;          /* 1: constant pressure (plugin option constant_volume = 0) */
+  double dpdt;     /* pressure rate (Pa/s), ZERORK_FIELD_DPDT */
+  double e_src;    /* energy source (J/kg/s), ZERORK_FIELD_E_SRC */
+  double P0, T0;   /* pressure_ and initial_temperature_ */
+  double E0;       /* initial_energy_: mass u (constant volume) or h (constant pressure) */
+  double time;     /* time argument of the next evaluation, from the start of the call */
   double *lim, *C, *net, *cre, *des, *rop, *u_RT, *cv_spc, mean_cv;
   double *tmp1, *tmp2, *tmp3;
   double *yscale;  /* [nsp+1] rounding scale of the last ydot: sum of |terms| */
@@ -113,10 +132,34 @@ zo_reactor *zo_reactor_new(const zo_tables *t, const zo_kinetics *kin,
 void zo_reactor_free(zo_reactor *r);
 /* Density from (T, P, Y): sets inv_density. */
 void zo_reactor_set_density(zo_reactor *r, double T, double P, const double *Y);
+/* InitializeState at time 0 (reactor_constant_volume_cpu.cpp:15-41,
+ * reactor_constant_pressure_cpu.cpp:15-41): density, initial energy and the
+ * sources; r->cp selects the reactor. */
+void zo_reactor_init_state(zo_reactor *r, double T, double P, const double *Y, double dpdt,
+                           double e_src, const double *y_src);
+/* GetState's pressure at time t for the end state (T, Y)
+ * (reactor_constant_volume_cpu.cpp:59, reactor_constant_pressure_cpu.cpp:59-63). */
+double zo_reactor_pressure(const zo_reactor *r, double t, double T, const double *Y);
 
-/* ydot for y = [Y, T/Tref]: reactor_constant_volume_cpu.cpp:64-128.
- * Returns 1 if T <= 0 (line 83). */
-int zo_cv_rhs(zo_reactor *r, const double *y, double *ydot);
+/* ydot for y = [Y, T/Tref] at time r->time: GetTimeDerivative of
+ * reactor_constant_volume_cpu.cpp:64-128 or reactor_constant_pressure_cpu.cpp:
+ * 71-135.  Returns 1 if T <= 0. */
+int zo_reactor_rhs(zo_reactor *r, const double *y, double *ydot);
+
+/* Mixture thermodynamics through a kinetics provider (test hook), per state
+ * s (Y reactor-major [n][nsp]): out[7s .. 7s+6] = density(T, P, Y),
+ * pressure(T, 1/density, Y), mass u(T, Y), mass h(T, Y), mass c_p(T, Y),
+ * T from (E[s], Y) and T from (H[s], Y), both with guess T[s]. */
+void zo_mix_thermo(const zo_kinetics *k, int nsp, int n, const double *T, const double *P,
+                   const double *Y, const double *E, const double *H, double *out);
+/* GetTimeDerivative over states (test hook): reactor s initialised at
+ * (T0, P0, Y0) with sources dpdt, e_src and y_src (each may be NULL), then
+ * ydot at time tm[s] and state y[s] ([n][nsp+1] both).  cp selects the
+ * constant-pressure reactor.  Returns the number of failed evaluations. */
+int zo_reactor_rhs_batch(const zo_tables *t, const zo_kinetics *k, int cp, int n,
+                         const double *T0, const double *P0, const double *Y0,
+                         const double *dpdt, const double *e_src, const double *y_src,
+                         const double *tm, const double *y, double *ydot);
 
 /* Fixed Jacobian pattern: reactor_nvector_serial.cpp:122-281
  * (SetupSparseJacobianArrays), CSC over n = nsp+1 variables. */

@@ -58,7 +58,13 @@ class ZoBdfOpts(C.Structure):
                 ("nlscoef", C.c_double), ("max_steps", C.c_int), ("Tref", C.c_double),
                 ("min_mass_frac", C.c_double), ("step_limiter", C.c_double),
                 ("analytic", C.c_int), ("max_retries", C.c_int), ("retry_atol", C.c_double),
-                ("retry_rtol", C.c_double), ("dT_ign", C.c_double)]
+                ("retry_rtol", C.c_double), ("dT_ign", C.c_double),
+                ("constant_volume", C.c_int)]
+
+
+class ZoKinetics(C.Structure):
+    """zo_kinetics: a context pointer and 12 function pointers (opaque here)."""
+    _fields_ = [("p%d" % i, C.c_void_p) for i in range(13)]
 
 
 class ZoBdfStats(C.Structure):
@@ -104,6 +110,11 @@ def _bind_common(lib):
                                        C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.zo_batch_rates_jac.restype = C.c_int
     lib.zo_kinetics_oracle.argtypes = [C.POINTER(ZoTables), C.c_void_p]
+    lib.zo_mix_thermo.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+    lib.zo_reactor_rhs_batch.argtypes = [C.POINTER(ZoTables), C.c_void_p, C.c_int, C.c_int, _dp,
+                                         _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p, _dp, _dp,
+                                         _dp]
+    lib.zo_reactor_rhs_batch.restype = C.c_int
     lib.zo_batch_rates_jac_scaled.argtypes = [C.POINTER(ZoTables), C.POINTER(ZoJacPattern),
                                               C.c_int, _dp, _dp, _dp, C.c_double, C.c_double,
                                               C.c_double, _dp, _dp, _dp, _dp]
@@ -112,7 +123,8 @@ def _bind_common(lib):
         lib.zo_bdf_default_opts.argtypes = [C.POINTER(ZoBdfOpts)]
         lib.zo_reactor_solve_batch.argtypes = [C.POINTER(ZoTables), C.POINTER(ZoJacPattern),
                                                C.POINTER(ZoBdfOpts), C.c_int, C.c_int, C.c_double,
-                                               _dp, _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p]
+                                               _dp, _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.c_void_p]
         lib.zo_reactor_solve_batch.restype = C.c_int
     return lib
 
@@ -153,12 +165,40 @@ def ref_lib(kind="libc"):
                                                C.c_double, C.c_double, C.c_double,
                                                C.c_void_p, C.c_void_p, C.c_void_p]
         lib.zrkref_batch_rates_jac.restype = C.c_int
+        lib.zrkref_mix_thermo.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp]
+        lib.zrkref_reactor_rhs_batch.argtypes = [C.c_void_p, C.POINTER(ZoTables), C.c_int, C.c_int,
+                                                 _dp, _dp, _dp, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, _dp, _dp, _dp]
+        lib.zrkref_reactor_rhs_batch.restype = C.c_int
         _refs[kind] = lib
     return _refs[kind]
 
 
 def _vp(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _mix_thermo(fn, kin, nsp, T, P, Y, E, H):
+    T, P, E, H = (np.ascontiguousarray(a, dtype=np.float64) for a in (T, P, E, H))
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    n = T.shape[0]
+    out = np.zeros((n, 7))
+    fn(kin, nsp, n, T, P, Y, E, H, out)
+    return out
+
+
+def _reactor_rhs(fn, nsp, cp, T0, P0, Y0, tm, y, dpdt, e_src, y_src):
+    T0, P0, tm = (np.ascontiguousarray(a, dtype=np.float64) for a in (T0, P0, tm))
+    Y0 = np.ascontiguousarray(Y0, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    dp, es, ys = (None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                  for a in (dpdt, e_src, y_src))
+    n = T0.shape[0]
+    ydot = np.zeros((n, nsp + 1))
+    nf = fn(int(cp), n, T0, P0, Y0, _vp(dp), _vp(es), _vp(ys), tm, y, ydot)
+    if nf:
+        raise RuntimeError(f"reactor rhs failed on {nf} states")
+    return ydot
 
 
 def tables_to_dict(tp):
@@ -243,7 +283,7 @@ class OracleTables:
         wdot = np.zeros((ns, self.nsp))
         jac = np.zeros((ns, nnz)) if want_jac else None
         ydot = np.zeros((ns, self.nsp + 1)) if want_ydot else None
-        kin_sz = 8 * 6
+        kin_sz = C.sizeof(ZoKinetics)
         kins = (C.c_char * (kin_sz * nthreads))()
         for i in range(nthreads):
             self.lib.zo_kinetics_oracle(self.ptr, C.cast(C.byref(kins, kin_sz * i), C.c_void_p))
@@ -270,11 +310,28 @@ class OracleTables:
         return wdot, jac, ws, js
 
 
-    def solve(self, T, P, Y, dt, nthreads=1, y_src=None, **opts):
-        """Oracle BDF integration of constant-volume reactors (reactor-major Y).
-        y_src: optional [n, nsp] mass-fraction source terms.  Returns (T, P,
-        Y, stats-dict-of-arrays); stats["t_ign"] holds the ignition times
-        when opts sets dT_ign > 0 (-1 where not reached).  opts override the
+    def mix_thermo(self, T, P, Y, E, H):
+        """Per state: density, pressure(T, 1/density), mass u, mass h, mass
+        c_p, T from (E, Y) and T from (H, Y) (guess T), on the restatement."""
+        k = ZoKinetics()
+        self.lib.zo_kinetics_oracle(self.ptr, C.byref(k))
+        return _mix_thermo(self.lib.zo_mix_thermo, C.byref(k), self.nsp, T, P, Y, E, H)
+
+    def reactor_rhs(self, cp, T0, P0, Y0, tm, y, dpdt=None, e_src=None, y_src=None):
+        """GetTimeDerivative after InitializeState(T0, P0, Y0, sources), at
+        time tm and state y [n, nsp+1]; cp selects constant pressure."""
+        k = ZoKinetics()
+        self.lib.zo_kinetics_oracle(self.ptr, C.byref(k))
+        return _reactor_rhs(lambda *a: self.lib.zo_reactor_rhs_batch(self.ptr, C.byref(k), *a),
+                            self.nsp, cp, T0, P0, Y0, tm, y, dpdt, e_src, y_src)
+
+    def solve(self, T, P, Y, dt, nthreads=1, y_src=None, dpdt=None, e_src=None, **opts):
+        """Oracle BDF integration of reactors (reactor-major Y), constant
+        volume unless opts sets constant_volume=0.  y_src: optional [n, nsp]
+        mass-fraction source terms; dpdt, e_src: optional [n] pressure-rate
+        (Pa/s) and energy (J/kg/s) sources.  Returns (T, P, Y,
+        stats-dict-of-arrays); stats["t_ign"] holds the ignition times when
+        opts sets dT_ign > 0 (-1 where not reached).  opts override the
         plugin defaults."""
         o = ZoBdfOpts()
         self.lib.zo_bdf_default_opts(C.byref(o))
@@ -285,10 +342,11 @@ class OracleTables:
         Y = np.array(Y, dtype=np.float64, order="C")
         n = T.shape[0]
         st = (ZoBdfStats * n)()
-        ys = None if y_src is None else np.ascontiguousarray(y_src, dtype=np.float64)
+        ys, dp, es = (None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                      for a in (y_src, dpdt, e_src))
         tign = np.full(n, -1.0)
         self.lib.zo_reactor_solve_batch(self.ptr, self.pat, C.byref(o), nthreads, n, float(dt),
-                                        T, P, Y, None if ys is None else ys.ctypes.data,
+                                        T, P, Y, _vp(ys), _vp(dp), _vp(es),
                                         tign.ctypes.data, C.cast(st, C.c_void_p))
         stats = {f: np.array([getattr(st[i], f) for i in range(n)]) for f, _ in ZoBdfStats._fields_}
         stats["t_ign"] = tign
@@ -348,6 +406,18 @@ class RefMechanism:
         cp, h, g = np.zeros(n), np.zeros(n), np.zeros(n)
         self.lib.zrkref_thermo(self.h, float(T), cp, h, g)
         return cp, h, g
+
+    def mix_thermo(self, T, P, Y, E, H):
+        """As OracleTables.mix_thermo, on the reference's mechanism functions."""
+        return _mix_thermo(lambda *a: self.lib.zrkref_mix_thermo(self.h, *a[2:]), None,
+                           self.nsp, T, P, Y, E, H)
+
+    def reactor_rhs(self, otab, cp, T0, P0, Y0, tm, y, dpdt=None, e_src=None, y_src=None):
+        """As OracleTables.reactor_rhs, on the reference's mechanism functions
+        (the reactor assembly is the restatement's)."""
+        tp = C.cast(otab.ptr, C.POINTER(ZoTables))
+        return _reactor_rhs(lambda *a: self.lib.zrkref_reactor_rhs_batch(self.h, tp, *a),
+                            self.nsp, cp, T0, P0, Y0, tm, y, dpdt, e_src, y_src)
 
     def batch_rates_jac(self, mech_files, otab, T, P, Y, Tref=1.0, mmf=1e-30, lim=1e22,
                         nthreads=1, want_jac=True):

@@ -40,6 +40,9 @@ typedef struct zo_bdf_opts {
    * T0 + dT_ign (ReactorNVectorSerial::RootFunction, :774-784), located by
    * linear interpolation between the accepted steps that bracket it */
   double dT_ign;
+  /* constant_volume: 1 constant-volume reactor, 0 constant-pressure reactor
+   * (zerork_reactor_manager.cpp:85, :913-917) */
+  int constant_volume;
 } zo_bdf_opts;
 
 typedef struct zo_bdf_stats {
@@ -49,19 +52,24 @@ typedef struct zo_bdf_stats {
 
 void zo_bdf_default_opts(zo_bdf_opts *o);
 
-/* Integrate one constant-volume reactor from (T, P, Y) for dt seconds:
- * InitializeState / Integrate / GetState of the cfd_plugin
- * (reactor_constant_volume_cpu.cpp:15-61, zerork_reactor_manager.cpp:1090-1146).
- * On return T, P, Y hold the end state. */
+/* Integrate one reactor (constant volume or constant pressure, o->
+ * constant_volume) from (T, P, Y) for dt seconds: InitializeState /
+ * Integrate / GetState of the cfd_plugin (reactor_constant_volume_cpu.cpp:
+ * 15-61, reactor_constant_pressure_cpu.cpp:15-66, zerork_reactor_manager.cpp:
+ * 1090-1146), with optional mass-fraction sources y_src [nsp] (or NULL), a
+ * pressure rate dpdt (Pa/s) and an energy source e_src (J/kg/s).  On return
+ * T, P, Y hold the end state. */
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
                      const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
-                     const double *y_src, double *t_ign, zo_bdf_stats *st);
+                     const double *y_src, double dpdt, double e_src, double *t_ign,
+                     zo_bdf_stats *st);
 
 /* Batch over reactors (reactor-major Y [n][nsp]) with nthreads OpenMP
  * threads, one reactor object per thread; stats may be NULL. */
 int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
                            int nthreads, int n, double dt, double *T, double *P, double *Y,
-                           const double *y_src, double *t_ign, zo_bdf_stats *stats);
+                           const double *y_src, const double *dpdt, const double *e_src,
+                           double *t_ign, zo_bdf_stats *stats);
 
 #ifdef __cplusplus
 }

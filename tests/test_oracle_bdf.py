@@ -16,17 +16,19 @@ from conftest import oracle_tables, synth
 
 
 def _rhs_and_jac(ot, T0, P0, Y0):
+    import zrk_oracle as zo
     L = ot.lib
-    kin = (C.c_char * 48)()
-    L.zo_kinetics_oracle(ot.ptr, C.cast(kin, C.c_void_p))
+    kin = zo.ZoKinetics()
+    L.zo_kinetics_oracle(ot.ptr, C.byref(kin))
     L.zo_reactor_new.restype = C.c_void_p
-    L.zo_reactor_new.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double]
+    L.zo_reactor_new.argtypes = [C.c_void_p, C.POINTER(zo.ZoKinetics), C.c_double, C.c_double,
+                                 C.c_double]
     L.zo_reactor_free.argtypes = [C.c_void_p]
     L.zo_reactor_set_density.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p]
-    L.zo_cv_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.zo_reactor_rhs.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     L.zo_jac_values.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p]
-    r = L.zo_reactor_new(ot.ptr, kin, 1.0, 1e-30, 1e22)
+    r = L.zo_reactor_new(ot.ptr, C.byref(kin), 1.0, 1e-30, 1e22)
     Y0 = np.ascontiguousarray(Y0, dtype=np.float64)
     L.zo_reactor_set_density(r, T0, P0, Y0.ctypes.data)
     pat = ot.pat.contents
@@ -37,7 +39,7 @@ def _rhs_and_jac(ot, T0, P0, Y0):
     def f(t, y):
         y = np.ascontiguousarray(y, dtype=np.float64)
         out = np.zeros(n)
-        assert L.zo_cv_rhs(r, y.ctypes.data, out.ctypes.data) == 0
+        assert L.zo_reactor_rhs(r, y.ctypes.data, out.ctypes.data) == 0
         return out
 
     def jac(t, y):

@@ -67,6 +67,82 @@ def test_oracle_batch_jacobian_on_reference_rates(tmp_path):
     np.testing.assert_array_equal(j1, j2)
 
 
+def _src_states(g, n, seed):
+    """States, energies and sources for the constant-pressure / source pins."""
+    from zerork_b200 import mechgen
+    T, P, Y = mechgen.rate_states(g, n, seed=seed)
+    rng = np.random.default_rng(seed)
+    return T, P, Y, rng
+
+
+@needs_ref
+@pytest.mark.parametrize("mech,therm", [
+    ("hydrogen/h2_v1b_mech.txt", "hydrogen/h2_v1a_therm.txt"),
+    ("dme/dme_24_mech.txt", "dme/dme_24_therm.txt"),
+])
+def test_mixture_thermo_matches_reference_library(mech, therm):
+    """Density, pressure, mass u / h / c_p and the T(E, Y) / T(H, Y) Newton
+    inversions (mechanism.cpp:279-547) equal the reference library's,
+    including the extrapolation below 100 K and above 5000 K."""
+    m, t = os.path.join(REF_DATA, mech), os.path.join(REF_DATA, therm)
+    if not (os.path.exists(m) and os.path.exists(t)):
+        pytest.skip("mechanism not shipped")
+    ref = zo.RefMechanism(m, t)
+    ot = zo.OracleTables(ref.tables)
+    rng = np.random.default_rng(3)
+    n = 200
+    T = rng.uniform(300, 3000, n)
+    P = 10 ** rng.uniform(4, 7, n)
+    Y = rng.dirichlet(np.full(ref.nsp, 0.5), n)
+    # energies of a temperature elsewhere in [20, 7000] K: Newton from T, and
+    # both extrapolations
+    T2 = np.concatenate([rng.uniform(150, 4900, n - 40), rng.uniform(20, 90, 20),
+                         rng.uniform(5100, 7000, 20)])
+    E = ot.mix_thermo(T2, P, Y, np.zeros(n), np.zeros(n))[:, 2]
+    H = ot.mix_thermo(T2, P, Y, np.zeros(n), np.zeros(n))[:, 3]
+    a = ref.mix_thermo(T, P, Y, E, H)
+    b = ot.mix_thermo(T, P, Y, E, H)
+    np.testing.assert_array_equal(a, b)
+    inner = (T2 > 100) & (T2 < 5000)
+    assert np.max(np.abs(b[inner, 5] - T2[inner])) < 1e-5
+    assert np.max(np.abs(b[inner, 6] - T2[inner])) < 1e-3  # c_v steps: slower, same root
+
+
+@needs_ref
+@pytest.mark.parametrize("cp", [0, 1])
+def test_reactor_rhs_sources_on_reference_functions(tmp_path, cp):
+    """The restated constant-volume / constant-pressure right-hand side with
+    DPDT, E_SRC and Y_SRC gives identical values on the oracle's and on the
+    reference library's mechanism functions."""
+    from zerork_b200 import mechgen
+    g = mechgen.generate(mechgen.SPECS["c1_h2"])
+    m, t = g.write(str(tmp_path))
+    ref = zo.RefMechanism(m, t)
+    ot = zo.OracleTables(ref.tables)
+    T, P, Y, rng = _src_states(g, 96, 7)
+    n, ns = len(T), ref.nsp
+    # sources that move P by ~1e4 Pa and T by ~30 K over tm (<= 1 ms)
+    dpdt = np.where(rng.uniform(size=n) < 0.5, rng.normal(0, 1e7, n), 0.0)
+    esrc = np.where(rng.uniform(size=n) < 0.5, rng.normal(0, 3e7, n), 0.0)
+    ysrc = rng.normal(0, 10.0, (n, ns))
+    tm = rng.uniform(0, 1e-3, n)
+    # small composition changes: at fixed energy, heats of formation turn a
+    # large one into a temperature outside the NASA-7 range
+    Yp = Y * rng.uniform(0.999, 1.001, (n, ns))
+    Yp /= Yp.sum(axis=1, keepdims=True)
+    y = np.concatenate([Yp, (T * rng.uniform(0.95, 1.05, n))[:, None]], axis=1)
+    for srcs in ({}, {"dpdt": dpdt}, {"e_src": esrc}, {"dpdt": dpdt, "e_src": esrc},
+                 {"dpdt": dpdt, "e_src": esrc, "y_src": ysrc}):
+        a = ref.reactor_rhs(ot, cp, T, P, Y, tm, y, **srcs)
+        b = ot.reactor_rhs(cp, T, P, Y, tm, y, **srcs)
+        np.testing.assert_array_equal(a, b)
+        assert np.all(np.isfinite(b))
+    # the sources act: without them the temperature derivative differs
+    base = ot.reactor_rhs(cp, T, P, Y, tm, y)
+    with_e = ot.reactor_rhs(cp, T, P, Y, tm, y, e_src=esrc)
+    assert np.all((with_e[:, ns] != base[:, ns]) == (esrc != 0))
+
+
 @pytest.mark.parametrize("name", ["c1_h2", "c2_53"])
 def test_oracle_against_golden(name, mech_dir):
     """Golden fixtures = reference-library outputs; regenerate with tests/golden/make_golden.py."""
