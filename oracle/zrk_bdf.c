@@ -56,6 +56,12 @@ typedef struct {
   double *jac;     /* nnz sparse values */
   double *A;       /* n x n dense Newton matrix, LU in place */
   double *Jd;      /* n x n dense divided-difference Jacobian (analytic = 0) */
+  /* energy source: the right-hand side takes T from the energy, T* =
+   * T(E0 + e_src t, Y), so it depends on Y through T* as well; the Newton
+   * matrix adds that coupling as the rank-one term g d^T with g = df/dT*
+   * and d_j = dT* by dY_j = -e_j / c_x (r1 = 1 when set) */
+  double *r1g, *r1d;
+  int r1;
   int *piv;
   double *y, *f, *f0, *ypred, *psi, *d, *dy, *scale, *rhs, *err, *tmp;
   double c_lu, crate;
@@ -110,6 +116,23 @@ static int take_jacobian(bdf_t *b, double t, const double *y, const double *f) {
   if (zo_jac_values(b->r, b->p, y, f, b->jac, NULL)) return 1;
   for (int i = 0; i < b->nnz; ++i)
     if (!isfinite(b->jac[i])) return 1;
+  b->r1 = 0;
+  if (b->r->e_src != 0.0) {
+    const int n = b->n, ns = n - 1;
+    double *f1 = b->tmp + n, *f2 = b->tmp + 2 * n;
+    if (rhs(b, t, y, f1)) return 1;
+    const double Ts = b->r->T_used, cx = b->r->mean_cv;
+    for (int j = 0; j < ns; ++j)
+      b->r1d[j] = -(b->r->u_RT[j] * (ZO_RU / b->r->t->mw[j] * Ts)) / cx;
+    b->r1d[ns] = 0.0;
+    const double Tp = Ts + Ts * sqrt(2.220446049250313e-16);
+    b->r->T_force = Tp;
+    const int bad = rhs(b, t, y, f2);
+    b->r->T_force = 0.0;
+    if (bad) return 1;
+    for (int i = 0; i < n; ++i) b->r1g[i] = (f2[i] - f1[i]) / (Tp - Ts);
+    b->r1 = 1;
+  }
   b->jac_current = 1;
   return 0;
 }
@@ -126,6 +149,9 @@ static int factor(bdf_t *b, double c) {
       for (int k = b->p->col_ptr[j]; k < b->p->col_ptr[j + 1]; ++k)
         A[b->p->row_idx[k] * n + j] = -c * b->jac[k];
   }
+  if (b->o->analytic && b->r1)
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) A[i * n + j] -= c * b->r1g[i] * b->r1d[j];
   for (int i = 0; i < n; ++i) A[i * n + i] += 1.0;
   for (int k = 0; k < n; ++k) {
     int pr = k;
@@ -390,6 +416,8 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   b.y = w; b.f = w + n; b.f0 = w + 2 * n; b.ypred = w + 3 * n; b.psi = w + 4 * n;
   b.d = w + 5 * n; b.dy = w + 6 * n; b.scale = w + 7 * n; b.rhs = w + 8 * n; b.err = w + 9 * n;
   b.tmp = w + 10 * n;
+  b.r1g = (double *)calloc((size_t)2 * n, sizeof(double));
+  b.r1d = b.r1g + n;
   double *y = (double *)calloc(n, sizeof(double));
   b.r->cp = o->constant_volume == 0;
   zo_reactor_init_state(b.r, *T, *P, Y, dpdt, e_src, y_src);
@@ -425,7 +453,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
     *P = zo_reactor_pressure(b.r, dt, *T, Y);
   }
   if (st) *st = b.st;
-  free(y); free(w); free(b.piv); free(b.A); free(b.Jd); free(b.jac); free(b.D);
+  free(y); free(w); free(b.r1g); free(b.piv); free(b.A); free(b.Jd); free(b.jac); free(b.D);
   zo_reactor_free(b.r);
   return rc;
 }

@@ -431,11 +431,13 @@ int zo_reactor_rhs(zo_reactor *r, const double *y, double *ydot) {
       r->inv_density = 1.0 / r->kin.density_TPY(r->kin.ctx, T, Pc, y);
       v = r->inv_density;
     }
-    if (r->e_src != 0.0) T = r->kin.temp_from_HY(r->kin.ctx, r->E0 + r->e_src * dt, y, T);
+    if (r->T_force > 0.0) T = r->T_force;
+    else if (r->e_src != 0.0) T = r->kin.temp_from_HY(r->kin.ctx, r->E0 + r->e_src * dt, y, T);
     r->kin.enthalpy_RT(r->kin.ctx, T, r->u_RT);
     r->mean_cv = r->kin.mass_cp(r->kin.ctx, T, y, r->cv_spc);
   } else {
-    if (r->e_src != 0.0) T = r->kin.temp_from_EY(r->kin.ctx, r->E0 + r->e_src * dt, y, T);
+    if (r->T_force > 0.0) T = r->T_force;
+    else if (r->e_src != 0.0) T = r->kin.temp_from_EY(r->kin.ctx, r->E0 + r->e_src * dt, y, T);
     r->kin.int_energy_RT(r->kin.ctx, T, r->u_RT);
     r->mean_cv = r->kin.mass_cv(r->kin.ctx, T, y, r->cv_spc);
     if (r->dpdt != 0.0) {
@@ -443,6 +445,7 @@ int zo_reactor_rhs(zo_reactor *r, const double *y, double *ydot) {
       v = 1.0 / r->kin.density_TPY(r->kin.ctx, T, Pc, y);
     }
   }
+  r->T_used = T;
   r->kin.c_from_vy(r->kin.ctx, v, y, r->C);
   r->kin.rates_limiter(r->kin.ctx, T, r->C, r->lim, r->net, r->cre, r->des, r->rop);
   double esum = 0.0;

@@ -120,6 +120,9 @@ typedef struct zo_reactor {
   double P0, T0;   /* pressure_ and initial_temperature_ */
   double E0;       /* initial_energy_: mass u (constant volume) or h (constant pressure) */
   double time;     /* time argument of the next evaluation, from the start of the call */
+  double T_force;  /* > 0: evaluate at this temperature instead of the state's or the
+                      energy source's (a finite-difference hook of the integrator) */
+  double T_used;   /* temperature the last evaluation used */
   double *lim, *C, *net, *cre, *des, *rop, *u_RT, *cv_spc, mean_cv;
   double *tmp1, *tmp2, *tmp3;
   double *yscale;  /* [nsp+1] rounding scale of the last ydot: sum of |terms| */

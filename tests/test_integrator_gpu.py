@@ -156,19 +156,96 @@ def test_ignition_time(gpu, mech_dir):
     assert np.all(ign[~hit] == -1.0)
 
 
-def test_unsupported_sources_refused(gpu, mech_dir):
-    """Non-zero DPDT / E_SRC sources are refused (not silently ignored)."""
+def _src_case(g, pm, n, seed):
+    """C1 reactors with pressure-rate, energy and mass-fraction sources; a
+    quarter of the reactors have none."""
     from zerork_b200 import mechgen
+    T, P, Y = mechgen.reactor_states(g, n, "c1", seed=seed)
+    rng = np.random.default_rng(seed)
+    on = rng.uniform(size=n) >= 0.25
+    dpdt = np.where(on, rng.uniform(-1e6, 1e7, n), 0.0)       # up to 0.1 bar per ms
+    esrc = np.where(on, rng.uniform(-1e8, 1e8, n), 0.0)       # up to ~100 K per ms
+    ys = np.zeros_like(Y)
+    ys[:, pm.species.index("N2")] = np.where(on, 5.0, 0.0)
+    return T, P, Y, dpdt, esrc, ys
+
+
+@pytest.mark.parametrize("cv,method,fp32,ysrc", [(1, 1, 0, False), (0, 1, 0, False),
+                                                 (1, 2, 0, False), (0, 2, 0, False),
+                                                 (0, 1, 0, True), (1, 1, 0, True),
+                                                 (1, 1, 1, False), (0, 2, 1, False)])
+def test_pressure_energy_sources_and_constant_pressure(gpu, cv, method, fp32, ysrc, mech_dir):
+    """Constant-volume (constant_volume = 1) and constant-pressure
+    (constant_volume = 0) reactors with ZERORK_FIELD_DPDT and ZERORK_FIELD_E_SRC
+    sources (reactor_constant_volume_cpu.cpp:64-128,
+    reactor_constant_pressure_cpu.cpp:71-135), optionally with Y_SRC, on both
+    integrators and both precisions, against the oracle with the same
+    sources: end T, P and Y within the integration-tolerance bound of the
+    module docstring.  The reference run is at rtol 1e-10: with an energy
+    source the right-hand side takes T from the reference's energy inversion,
+    which stops at 1e-6 K, and tighter runs stall on that noise."""
     from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
     g, (mf, tf) = synth("c1_h2", mech_dir)
-    T, P, Y = mechgen.reactor_states(g, 4, "c1", seed=2)
-    p = Plugin(mf, tf)
-    p.set_aux_field("DPDT", np.zeros(4))
-    assert p.solve(1e-4, T.copy(), P.copy(), Y.copy()) == 0
-    p.set_aux_field("E_SRC", np.array([0.0, 0.0, 1.0, 0.0]))
-    from zerork_b200.plugin import PluginError
-    with pytest.raises(PluginError):
-        p.solve(1e-4, T.copy(), P.copy(), Y.copy())
+    pm = zb.Mechanism(mf, tf, device=False)
+    n, dt = 16, 1e-3
+    T, P, Y, dpdt, esrc, ys = _src_case(g, pm, n, 21 + cv + 2 * method)
+    p = Plugin(mf, tf, constant_volume=cv, gpu_method=method, lu_fp32=fp32)
+    p.set_aux_field("DPDT", dpdt)
+    p.set_aux_field("E_SRC", esrc)
+    if ysrc:
+        p.set_aux_field("Y_SRC", ys)
+    Tg, Pg, Yg = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert p.solve(dt, Tg, Pg, Yg) == 0
+    ot = oracle_tables(pm)
+    nt = os.cpu_count() or 1
+    src = dict(dpdt=dpdt, e_src=esrc, y_src=ys if ysrc else None, constant_volume=cv)
+    To, Po, Yo, so = ot.solve(T, P, Y, dt, nthreads=nt, **src)
+    Tt, Pt, Yt, st = ot.solve(T, P, Y, dt, nthreads=nt, rtol=1e-10, atol=1e-22, max_steps=400000,
+                              **src)
+    ok = (so["status"] == 0) & (st["status"] == 0)
+    assert ok.sum() >= n - 2
+    for g_, o_, t_, rel in ((Tg, To, Tt, 1e-5), (Pg, Po, Pt, 1e-8)):
+        eo, eg = np.abs(o_ - t_)[ok], np.abs(g_ - t_)[ok]
+        assert np.all(eg <= 50 * np.maximum(eo, 10 * np.median(eo)) + rel * np.abs(t_[ok])), (eg, eo)
+    eo_Y, eg_Y = np.max(np.abs(Yo - Yt), axis=1)[ok], np.max(np.abs(Yg - Yt), axis=1)[ok]
+    assert np.all(eg_Y <= 50 * np.maximum(eo_Y, 10 * np.median(eo_Y)) + 1e-8)
+    # at constant pressure without mass sources the end pressure is P0 + dpdt dt
+    if cv == 0 and not ysrc:
+        assert np.allclose(Pg, P + dpdt * dt, rtol=1e-14, atol=0.0)
+    # the energy source acts: against a run without it, the end temperature
+    # moves the way the source points
+    Tn, Pn, Yn = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    q = Plugin(mf, tf, constant_volume=cv, gpu_method=method, lu_fp32=fp32)
+    q.set_aux_field("DPDT", dpdt)
+    if ysrc:
+        q.set_aux_field("Y_SRC", ys)
+    assert q.solve(dt, Tn, Pn, Yn) == 0
+    big = np.abs(esrc) > 1e7
+    assert np.all(np.sign(Tg - Tn)[big] == np.sign(esrc)[big])
+
+
+def test_constant_pressure_c3_subset(gpu, mech_dir):
+    """Constant-pressure C3 reactors (160 species, dense integrator) without
+    sources: end state against the oracle, pressure unchanged."""
+    from zerork_b200 import mechgen
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c3_160", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 6, "c3", seed=5)
+    rc, Tg, Pg, Yg, p = _solve(mf, tf, T, P, Y, 2e-4, constant_volume=0)
+    assert rc == 0
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    nt = os.cpu_count() or 1
+    To, Po, Yo, so = ot.solve(T, P, Y, 2e-4, nthreads=nt, constant_volume=0)
+    Tt, Pt, Yt, st = ot.solve(T, P, Y, 2e-4, nthreads=nt, constant_volume=0, rtol=1e-12, atol=1e-24,
+                              max_steps=400000)
+    ok = (so["status"] == 0) & (st["status"] == 0)
+    assert ok.sum() >= 3
+    eo_T, eg_T = np.abs(To - Tt)[ok], np.abs(Tg - Tt)[ok]
+    assert np.all(eg_T <= 50 * np.maximum(eo_T, 10 * np.median(eo_T)) + 1e-5 * Tt[ok])
+    eo_Y, eg_Y = np.max(np.abs(Yo - Yt), axis=1)[ok], np.max(np.abs(Yg - Yt), axis=1)[ok]
+    assert np.all(eg_Y <= 50 * np.maximum(eo_Y, 10 * np.median(eo_Y)) + 1e-8)
+    assert np.array_equal(Pg, P)
 
 
 def test_failure_leaves_state_and_reports(gpu, mech_dir):

@@ -1,5 +1,5 @@
-// integrator.cu -- warp-per-reactor BDF integration of constant-volume
-// reactors (see integrator.h).
+// integrator.cu -- warp-per-reactor BDF integration of constant-volume and
+// constant-pressure reactors (see integrator.h).
 //
 // Per warp: the reactor's right-hand side (reactor_constant_volume_cpu.cpp:
 // 64-128) with lanes over species and reactions; its Jacobian
@@ -13,6 +13,7 @@
 
 #include "integrator.h"
 #include "kinetics_dev.cuh"
+#include "reactor_src.cuh"
 
 namespace zrk {
 namespace {
@@ -33,6 +34,13 @@ struct Warp {
   double *C, *G, *U, *ROP;  // species rows and rates of progress
   void *X;                  // LU work / solve vector (n elements of the LU type)
   const double *ysrc;       // this reactor's mass-fraction sources (global) or null
+  ReactorSrc src;           // this reactor's pressure-rate / energy sources and initial state
+};
+
+// What one right-hand-side evaluation used: mixture heat capacity (c_v, or
+// c_p for constant pressure), temperature and inverse density.
+struct RhsOut {
+  double cx, T, v;
 };
 
 struct BdfConst {
@@ -51,16 +59,27 @@ __device__ void bdf_consts(BdfConst &b) {
   }
 }
 
-// ydot at y (global or shared vector of nsp+1 entries); returns 1 if T <= 0.
-__device__ int rhs_warp(const DevMech &m, const IntegOpts &o, const Warp &w, double v,
-                        const double *y, double *ydot, int lane, bool clamp, double *cv_out) {
+// ydot at y (global or shared vector of nsp+1 entries) and time t from the
+// start of the call; v0 is the reactor's initial inverse density.  Returns 1
+// if T <= 0.  Constant pressure (o.cp): reactor_constant_pressure_cpu.cpp:
+// 71-135, U then holds h/RT.  T_force > 0 replaces the energy-source
+// temperature (reactor_src.cuh).
+__device__ __forceinline__ int rhs_warp(const DevMech &m, const IntegOpts &o, const Warp &w,
+                                        double v0, double t, const double *y, double *ydot,
+                                        int lane, bool clamp, RhsOut *out,
+                                        double T_force = 0.0) {
   const int S = m.nsp;
   const double yS = y[S];
   double T = yS * o.Tref;
   if (!(T > 0.0)) return 1;
   if (T > 1.0e4) T = 1.0e4;
+  double v = v0;
+  if (o.cp || w.src.dpdt != 0.0 || w.src.esrc != 0.0)
+    source_T_v(m, o.cp != 0, w.src, t, y, clamp, o.mmf, v0, T_force, lane, 32,
+               [](double x) { return wsum(x); }, T, v);
   const double logT = log(T), invT = 1.0 / T, lprt = log(kPatmD / (kRuD * T));
   const double dens = 1.0 / v;
+  const double ush = o.cp ? 0.0 : 1.0;  // h/RT - 1 = u/RT; c_p/R - 1 = c_v/R
   double pc = 0.0, pcv = 0.0;
   for (int s = lane; s < S; s += 32) {
     double ys = y[s];
@@ -70,9 +89,9 @@ __device__ int rhs_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
     double cp, h, g;
     nasa_cp_h_g(m.thermo + 16 * s, T, logT, &cp, &h, &g);
     w.G[s] = g;
-    w.U[s] = h - 1.0;
+    w.U[s] = h - ush;
     pc += c;
-    pcv += ((cp - 1.0) * m.ru_inv_mw[s]) * ys;
+    pcv += ((cp - ush) * m.ru_inv_mw[s]) * ys;
   }
   const double Csum = wsum(pc), cv = wsum(pcv);
   __syncwarp();
@@ -95,29 +114,33 @@ __device__ int rhs_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
     }
   }
   const double es = wsum(pe);
-  if (lane == 0) ydot[S] = -es * kRuD * yS / cv + 0.0;
-  if (cv_out) *cv_out = cv;
+  if (lane == 0) ydot[S] = -es * kRuD * yS / cv + (w.src.esrc + w.src.dpdt * v) / (cv * o.Tref);
+  if (out) *out = RhsOut{cv, T, v};
   __syncwarp();
   return 0;
 }
 
-// Jacobian values J[nnz] at y with fy = ydot(y); tmp: nsp+1 global doubles,
-// yp: nsp+1 shared/global doubles of scratch.
-__device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, double v,
+// Jacobian values J[nnz] at y with fy = ydot(t, y); tmp: nsp+1 global
+// doubles, yp: nsp+1 shared/global doubles of scratch.  Concentration
+// derivatives use the initial inverse density at constant volume and the
+// current one at constant pressure.  Under an energy source, the rank-one
+// temperature coupling g = df/dT*, d = dT*/dY goes to r1g / r1d (see
+// integrator_dense.cuh's jac_cta).
+__device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, double v0, double t,
                         const double *y, const double *fy, double *J, double *tmp, double *yp,
-                        int lane) {
+                        double *r1g, double *r1d, int lane) {
   const int S = m.nsp;
   int need = 0;
   for (int s = lane; s < S; s += 32) need |= (fabs(y[s]) < o.mmf);
   need = __any_sync(kFull, need);
-  double cvc;
-  if (rhs_warp(m, o, w, v, y, tmp, lane, need != 0, &cvc)) return 1;
+  RhsOut ro;
+  if (rhs_warp(m, o, w, v0, t, y, tmp, lane, need != 0, &ro)) return 1;
   const double TdC = tmp[S];
   const double yS = y[S];
   const double RuTemp = kRuD * yS;
-  const double multFact = -1.0 / cvc;
-  double T = yS * o.Tref;
-  if (T > 1.0e4) T = 1.0e4;
+  const double multFact = -1.0 / ro.cx;
+  const double T = ro.T, v = o.cp ? ro.v : v0;
+  const double ush = o.cp ? 0.0 : 1.0;
   for (int j = 0; j < S; ++j) {
     const double t2 = m.mw[j] / clamp_mass_fraction(y[j], o.mmf) * v;
     const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
@@ -134,7 +157,7 @@ __device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
     }
     trow = wsum(trow);
     if (lane == 0) {
-      const double cvj = (nasa_cp(m.thermo + 16 * j, T) - 1.0) * m.ru_inv_mw[j];
+      const double cvj = (nasa_cp(m.thermo + 16 * j, T) - ush) * m.ru_inv_mw[j];
       double tr = trow * RuTemp;
       tr += TdC * cvj * m.mw[j];
       tr *= wcol * multFact;
@@ -148,12 +171,26 @@ __device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
   for (int s = lane; s < S; s += 32) yp[s] = y[s];
   if (lane == 0) yp[S] = ySp;
   __syncwarp();
-  if (rhs_warp(m, o, w, v, yp, tmp, lane, false, nullptr)) return 1;
+  if (rhs_warp(m, o, w, v0, t, yp, tmp, lane, false, nullptr)) return 1;
   for (int kk = m.col_ptr[S] + lane; kk < m.col_ptr[S + 1]; kk += 32) {
     const int row = m.row_idx[kk];
     J[kk] = (tmp[row] - fy[row]) * mult;
   }
   __syncwarp();
+  if (w.src.esrc != 0.0) {
+    RhsOut r1;
+    if (rhs_warp(m, o, w, v0, t, y, yp, lane, false, &r1)) return 1;
+    for (int j = lane; j < S; j += 32) {
+      double cpR, hRT;
+      nasa_cp_h(m.thermo + 16 * j, r1.T, &cpR, &hRT);
+      r1d[j] = -((hRT - ush) * (m.ru_inv_mw[j] * r1.T)) / r1.cx;
+    }
+    if (lane == 0) r1d[S] = 0.0;
+    const double Tp = r1.T + r1.T * o.sqrt_ur;
+    if (rhs_warp(m, o, w, v0, t, y, tmp, lane, false, nullptr, Tp)) return 1;
+    for (int i = lane; i <= S; i += 32) r1g[i] = (tmp[i] - yp[i]) / (Tp - r1.T);
+    __syncwarp();
+  }
   return 0;
 }
 
@@ -270,7 +307,18 @@ struct Vecs {
   double *D, *y, *f, *f0, *ypred, *psi, *d, *scale, *tmp, *J;
   double *wsc;  // scale the stored factor was formed with
   double *K;    // FP32 path: (kMaxl + 1) Krylov vectors, then 2 work vectors
+  double *r1g, *r1d, *r1w;  // energy-source coupling: g, d, w = P^-1 g
 };
+
+// Energy-source coupling on a Newton solve x = P^-1 b (Sherman-Morrison):
+// (P - c g d^T)^-1 b = x + w (r1k d.x), w = P^-1 g, r1k = c / (1 - c d.w).
+__device__ void rank1_fix_warp(const Vecs &V, int n, double r1k, double *x, int lane) {
+  double a = 0.0;
+  for (int i = lane; i < n; i += 32) a += V.r1d[i] * x[i];
+  const double dx = wsum(a) * r1k;
+  for (int i = lane; i < n; i += 32) x[i] += V.r1w[i] * dx;
+  __syncwarp();
+}
 
 constexpr int kMaxl = 10;  // Krylov dimension (no restarts)
 
@@ -281,14 +329,17 @@ constexpr int kMaxl = 10;  // Krylov dimension (no restarts)
 // converged when the preconditioned residual's weighted 2-norm is <= delta),
 // as the reference plugin drives it through CVODE (solver_cvode.cpp:119-141,
 // 201-212), restated from Saad and Schultz, SIAM J. Sci. Stat. Comput. 7
-// (1986) 856-869.  Every lane keeps the same Hessenberg matrix.  Returns 0
-// when converged, 1 otherwise.
+// (1986) 856-869.  Every lane keeps the same Hessenberg matrix.  Under an
+// energy source the operator and the preconditioner carry the rank-one
+// temperature coupling (r1 set).  Returns 0 when converged, 1 otherwise.
 template <class LT>
 __device__ int gmres_warp(const DevMech &m, const LUDev &lu, const Vecs &V, const LT *LU, LT *x, double c,
-                          double delta, const double *b, double *xo, int lane, int &iters) {
+                          double delta, const double *b, double *xo, int lane, int &iters,
+                          bool r1, double r1k) {
   const int n = lu.n;
   double *Kv = V.K, *u = V.K + (kMaxl + 1) * n, *z = u + n;
   precond_warp<LT>(lu, LU, x, V.wsc, b, z, lane);
+  if (r1) rank1_fix_warp(V, n, r1k, z, lane);
   double a = 0.0;
   for (int i = lane; i < n; i += 32) {
     const double t = z[i] / V.scale[i];
@@ -310,15 +361,22 @@ __device__ int gmres_warp(const DevMech &m, const LUDev &lu, const Vecs &V, cons
   for (int l = 0; l < kMaxl; ++l) {
     const double *vl = Kv + l * n;
     double *w = Kv + (l + 1) * n;
-    for (int i = lane; i < n; i += 32) u[i] = vl[i] * V.scale[i];
+    double du = 0.0;
+    for (int i = lane; i < n; i += 32) {
+      u[i] = vl[i] * V.scale[i];
+      if (r1) du += V.r1d[i] * u[i];
+    }
+    if (r1) du = wsum(du);
     __syncwarp();
     for (int i = lane; i < n; i += 32) {  // (I - cJ) u, row i
       double jx = 0.0;
       for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) jx += V.J[m.jr_kk[q]] * u[m.jr_col[q]];
+      if (r1) jx += V.r1g[i] * du;
       z[i] = u[i] - c * jx;
     }
     __syncwarp();
     precond_warp<LT>(lu, LU, x, V.wsc, z, z, lane);
+    if (r1) rank1_fix_warp(V, n, r1k, z, lane);
     for (int i = lane; i < n; i += 32) w[i] = z[i] / V.scale[i];
     __syncwarp();
     for (int k = 0; k <= l; ++k) {  // modified Gram-Schmidt
@@ -406,9 +464,19 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   int rc = 0;
   t_done = 0.0;
   double T_prev = V.y[m.nsp] * o.Tref;  // ignition: temperature at the last accepted step
+  const bool r1 = w.src.esrc != 0.0;
+  double r1k = 0.0;  // energy-source coupling of the current factor
+  auto rank1_setup = [&](double cc) {
+    if (!r1) return;
+    precond_warp<LT>(lu, LU, x, V.wsc, V.r1g, V.r1w, lane);
+    double a = 0.0;
+    for (int i = lane; i < n; i += 32) a += V.r1d[i] * V.r1w[i];
+    const double dw = wsum(a);
+    r1k = cc / (1.0 - cc * dw);
+  };
   // f0 = f(y0); initial step (Hairer-Norsett-Wanner)
   st.nrhs++;
-  if (rhs_warp(m, o, w, v, V.y, V.f0, lane, false, nullptr)) return -1;
+  if (rhs_warp(m, o, w, v, t_off, V.y, V.f0, lane, false, nullptr)) return -1;
   for (int i = lane; i < n; i += 32) V.scale[i] = atol + fabs(V.y[i]) * rtol;
   __syncwarp();
   const double d0 = wrms_scaled(V.y, V.scale, n, lane), d1 = wrms_scaled(V.f0, V.scale, n, lane);
@@ -418,7 +486,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   __syncwarp();
   double d2 = 0.0;
   st.nrhs++;
-  if (rhs_warp(m, o, w, v, V.tmp, V.f, lane, false, nullptr) == 0) {
+  if (rhs_warp(m, o, w, v, t_off + h0, V.tmp, V.f, lane, false, nullptr) == 0) {
     for (int i = lane; i < n; i += 32) V.d[i] = V.f[i] - V.f0[i];
     __syncwarp();
     d2 = wrms_scaled(V.d, V.scale, n, lane) / h0;
@@ -437,9 +505,10 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   }
   __syncwarp();
   st.njac++;
-  if (jac_warp(m, o, w, v, V.y, V.f0, V.J, V.tmp, V.d, lane)) { rc = -2; goto failed; }
+  if (jac_warp(m, o, w, v, t_off, V.y, V.f0, V.J, V.tmp, V.d, V.r1g, V.r1d, lane)) { rc = -2; goto failed; }
   st.nlu++;
   if (lu_factor_warp<LT>(m, lu, V.J, c_lu, V.scale, V.wsc, LU, x, lane)) { rc = -3; goto failed; }
+  rank1_setup(c_lu);
   while (t < t_end) {
     if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
@@ -472,6 +541,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         c_lu = c;
         crate = 1.0;
         if (lu_factor_warp<LT>(m, lu, V.J, c, V.scale, V.wsc, LU, x, lane)) { rc = -3; goto failed; }
+        rank1_setup(c);
       }
       const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
       bool conv = false;
@@ -479,7 +549,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       double dnorm_old = -1.0;
       for (it = 0; it < kNewtonMaxIter; ++it) {
         st.nrhs++;
-        if (rhs_warp(m, o, w, v, V.y, V.f, lane, false, nullptr)) break;
+        if (rhs_warp(m, o, w, v, t_off + t_new, V.y, V.f, lane, false, nullptr)) break;
         bool finite = true;
         for (int i = lane; i < n; i += 32) finite &= isfinite(V.f[i]);
         if (!__all_sync(kFull, finite)) break;
@@ -494,10 +564,12 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
           // tolerance eps_lin * nlscoef / error constant (WRMS); every solve
           // must converge (see integrator_dense.cuh)
           const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
-          if (gmres_warp<LT>(m, lu, V, LU, x, c, delta, V.tmp, V.tmp, lane, st.nkry) != 0) break;
+          if (gmres_warp<LT>(m, lu, V, LU, x, c, delta, V.tmp, V.tmp, lane, st.nkry, r1, r1k) != 0)
+            break;
           gs = 1.0;
         } else {
           precond_warp<LT>(lu, LU, x, V.wsc, V.tmp, V.tmp, lane);
+          if (r1) rank1_fix_warp(V, n, r1k, V.tmp, lane);
         }
         double a = 0.0;
         for (int i = lane; i < n; i += 32) {
@@ -521,14 +593,18 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       if (!conv) {
         if (!jac_current) {
           st.nrhs++;
-          if (rhs_warp(m, o, w, v, V.ypred, V.f0, lane, false, nullptr)) { rc = -6; goto failed; }
+          if (rhs_warp(m, o, w, v, t_off + t_new, V.ypred, V.f0, lane, false, nullptr)) { rc = -6; goto failed; }
           st.njac++;
-          if (jac_warp(m, o, w, v, V.ypred, V.f0, V.J, V.tmp, V.f, lane)) { rc = -2; goto failed; }
+          if (jac_warp(m, o, w, v, t_off + t_new, V.ypred, V.f0, V.J, V.tmp, V.f, V.r1g, V.r1d, lane)) {
+            rc = -2;
+            goto failed;
+          }
           jac_current = 1;
           st.nlu++;
           c_lu = c;
           crate = 1.0;
           if (lu_factor_warp<LT>(m, lu, V.J, c, V.scale, V.wsc, LU, x, lane)) { rc = -3; goto failed; }
+          rank1_setup(c);
           continue;
         }
         change_D(V.D, n, q, 0.5, lane);
@@ -660,6 +736,9 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     V.J = V.tmp + n;
     V.wsc = V.J + m.nnz;
     V.K = V.wsc + n;
+    V.r1g = V.K + (kMaxl + 3) * n;
+    V.r1d = V.r1g + n;
+    V.r1w = V.r1d + n;
     LT *LU = (LT *)a.lu + (size_t)r * a.lu_stride;
     // InitializeState (reactor_constant_volume_cpu.cpp:15-41)
     const double T0 = a.T[r], P0 = a.P[r];
@@ -668,6 +747,16 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     for (int s = lane; s < S; s += 32) pa += Y0[s] * m.inv_mw[s];
     const double mwmix = 1.0 / wsum(pa);
     const double v = 1.0 / (P0 * mwmix / (kRuD * T0));
+    w.src.dpdt = a.dpdt ? a.dpdt[r] : 0.0;
+    w.src.esrc = a.esrc ? a.esrc[r] : 0.0;
+    w.src.P0 = P0;
+    w.src.ysrc = a.ysrc != nullptr;
+    w.src.E0 = 0.0;
+    if (w.src.esrc != 0.0) {  // initial_energy_ (InitializeState)
+      double cx;
+      mix_energy(m, o.cp != 0, false, T0, Y0, false, 0.0, lane, 32,
+                 [](double x) { return wsum(x); }, w.src.E0, cx);
+    }
     for (int s = lane; s < S; s += 32) V.y[s] = Y0[s];
     if (lane == 0) V.y[S] = T0 / o.Tref;
     __syncwarp();
@@ -702,7 +791,7 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
       const double mw2 = 1.0 / wsum(pb);
       if (lane == 0) {
         a.T[r] = Tn;
-        a.P[r] = kRuD * Tn / (v * mw2);
+        a.P[r] = end_pressure(o.cp != 0, w.src, a.dt, Tn, mw2, v);
       }
     }
     if (lane == 0) {
@@ -723,7 +812,7 @@ size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem) 
 
 long integ_state_doubles(const DevMech &m, const LUDev &lu) {
   const long n = m.nsp + 1;
-  return (kMaxOrder + 3) * n + 8 * n + m.nnz + n + (kMaxl + 3) * n;
+  return (kMaxOrder + 3) * n + 8 * n + m.nnz + n + (kMaxl + 3) * n + 3 * n;
 }
 
 cudaError_t launch_integrate(const DevMech &m, const LUDev &lu, const IntegOpts &o,

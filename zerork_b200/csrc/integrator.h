@@ -1,6 +1,7 @@
 // integrator.h -- batched stiff reactor integration on sm_100a.
 //
-// One warp integrates one constant-volume reactor at a time with a
+// One warp integrates one reactor (constant volume, or constant pressure
+// with IntegOpts.cp) at a time with a
 // variable-order BDF (orders 1-5, quasi-constant step size, Shampine &
 // Reichelt 1997) and a modified Newton iteration with CVODE's convergence
 // test (Hindmarsh et al., ACM TOMS 2005), the Newton matrix I - cJ built from
@@ -44,6 +45,7 @@ struct IntegOpts {
   double retry_atol_factor, retry_rtol_factor;
   double Tref, mmf, lim, sqrt_ur;
   int lu_fp32;  // factor and apply the Newton matrix in FP32
+  int cp;       // 1: constant-pressure reactor (plugin option constant_volume = 0)
   double eps_lin;  // Krylov tolerance: eps_lin * nlscoef / error constant (WRMS)
   PredDev pred;    // learned predictor (dense integrator only; enabled = 0: off)
   double dT_ign;   // delta_temperature_ignition: > 0 records when T reaches T0 + dT_ign
@@ -71,6 +73,8 @@ struct IntegArgs {
   double *rop_scratch;      // optional global ROP rows (one per warp slot)
   const double *ysrc;       // optional mass-fraction sources [n_reactors][nsp] (1/s)
   double *t_ign;            // optional ignition times [n_reactors] (-1: not reached)
+  const double *dpdt;       // optional pressure rates [n_reactors] (Pa/s)
+  const double *esrc;       // optional energy sources [n_reactors] (J/kg/s)
 };
 
 size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);

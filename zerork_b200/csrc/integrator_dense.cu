@@ -18,7 +18,8 @@ size_t dense_smem_bytes(const DevMech &m, bool fp32, int *lda_out, int spill) {
 }
 
 size_t dense_spill_doubles(const DevMech &m) {
-  return (size_t)m.nstep + (kMaxOrder + 3) * (size_t)(m.nsp + 1);
+  // rates of progress, BDF differences, energy-source coupling vectors
+  return (size_t)m.nstep + (kMaxOrder + 6) * (size_t)(m.nsp + 1);
 }
 
 

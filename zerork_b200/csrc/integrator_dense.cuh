@@ -16,6 +16,7 @@
 
 #include "integrator.h"
 #include "kinetics_dev.cuh"
+#include "reactor_src.cuh"
 
 namespace zrk {
 namespace {
@@ -41,6 +42,16 @@ struct Smem {
   float *mlp;   // learned predictor: two activation buffers of kPredBuf floats
   double *Jsm;  // reactor Jacobian when it is kept in shared memory (spill bit 4)
   const double *ysrc;  // this reactor's mass-fraction sources (global) or null
+  ReactorSrc src;      // this reactor's pressure-rate / energy sources and initial state
+  // energy-source temperature coupling (global, n each): g = df/dT*,
+  // d = dT*/dY, w = (I - c J)^-1 g of the current factor
+  double *r1g, *r1d, *r1w;
+};
+
+// What one right-hand-side evaluation used: mixture heat capacity (c_v, or
+// c_p for constant pressure), temperature and inverse density.
+struct RhsOut {
+  double cx, T, v;
 };
 
 // Sum over the CTA; every thread gets thread 0's total (deterministic).
@@ -74,16 +85,33 @@ __device__ __forceinline__ double gather4(const double *v, const int *idx, int q
   return (a0 + a1) + (a2 + a3);
 }
 
-// ydot at y (shared vector); returns 1 if T <= 0 (all threads agree).
-__device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v,
-                       const double *y, double *ydot, bool clamp, double *cv_out) {
+// Source / constant-pressure adjustment of T and v (reactor_src.cuh).
+__device__ __forceinline__ void source_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
+                                           double t, const double *y, bool clamp, double v0,
+                                           double T_force, double &T, double &v) {
+  source_T_v(m, o.cp != 0, s.src, t, y, clamp, o.mmf, v0, T_force, threadIdx.x, blockDim.x,
+             [&](double x) { return block_sum(x, s.red); }, T, v);
+}
+
+// ydot at y (shared vector) and time t from the start of the call; v0 is the
+// reactor's initial inverse density.  Returns 1 if T <= 0 (all threads agree).
+// Constant volume: reactor_constant_volume_cpu.cpp:64-128; constant pressure
+// (o.cp): reactor_constant_pressure_cpu.cpp:71-135, U then holds h/RT.
+// T_force > 0 replaces the energy-source temperature.
+__device__ __forceinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
+                                       double v0, double t, const double *y, double *ydot,
+                                       bool clamp, RhsOut *out, double T_force = 0.0) {
   const int S = m.nsp, tid = threadIdx.x, nt = blockDim.x;
   const double yS = y[S];
   double T = yS * o.Tref;
   if (!(T > 0.0)) return 1;
   if (T > 1.0e4) T = 1.0e4;
+  double v = v0;
+  if (o.cp || s.src.dpdt != 0.0 || s.src.esrc != 0.0)
+    source_cta(m, o, s, t, y, clamp, v0, T_force, T, v);
   const double logT = log(T), invT = 1.0 / T, lprt = log(kPatmD / (kRuD * T));
   const double dens = 1.0 / v;
+  const double ush = o.cp ? 0.0 : 1.0;  // h/RT - 1 = u/RT; c_p/R - 1 = c_v/R
   double pc = 0.0, pcv = 0.0;
   for (int k = tid; k < S; k += nt) {
     double ys = y[k];
@@ -93,9 +121,9 @@ __device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
     double cp, h, g;
     nasa_cp_h_g(m.thermo + 16 * k, T, logT, &cp, &h, &g);
     s.G[k] = g;
-    s.U[k] = h - 1.0;
+    s.U[k] = h - ush;
     pc += c;
-    pcv += ((cp - 1.0) * m.ru_inv_mw[k]) * ys;
+    pcv += ((cp - ush) * m.ru_inv_mw[k]) * ys;
   }
   const double Csum = block_sum(pc, s.red);
   const double cv = block_sum(pcv, s.red);
@@ -124,27 +152,35 @@ __device__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
     }
   }
   const double es = block_sum(pe, s.red);
-  if (tid == 0) ydot[S] = -es * kRuD * yS / cv + 0.0;
-  if (cv_out) *cv_out = cv;
+  if (tid == 0) ydot[S] = -es * kRuD * yS / cv + (s.src.esrc + s.src.dpdt * v) / (cv * o.Tref);
+  if (out) *out = RhsOut{cv, T, v};
   __syncthreads();
   return 0;
 }
 
-// Reactor Jacobian (SetupJacobianSparse semantics) into J (global, nnz).
-__device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v,
-                       const double *y, const double *fy, double *J) {
-  const int S = m.nsp, tid = threadIdx.x, nt = blockDim.x;
+// Reactor Jacobian (SetupJacobianSparse semantics) into J (global, nnz) at
+// y with fy = ydot(t, y).  The concentration derivatives use the reactor's
+// inverse density: the initial one at constant volume, the current one at
+// constant pressure; the temperature row uses the heat capacities at the
+// temperature the right-hand side used.  Under an energy source the
+// right-hand side takes T from the energy, T* = T(E0 + esrc t, Y), which
+// this Jacobian does not see; the rank-one coupling g d^T (g = df/dT*,
+// d_j = dT*/dY_j = -e_j / c_x) goes to s.r1g / s.r1d for the Newton solves.
+__device__ __forceinline__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
+                                       double v0, double t, const double *y, const double *fy,
+                                       double *J) {
+  const int S = m.nsp, n = S + 1, tid = threadIdx.x, nt = blockDim.x;
   int need = 0;
   for (int k = tid; k < S; k += nt) need |= (fabs(y[k]) < o.mmf);
   need = __syncthreads_or(need);
-  double cvc;
-  if (rhs_cta(m, o, s, v, y, s.tmp, need != 0, &cvc)) return 1;
+  RhsOut ro;
+  if (rhs_cta(m, o, s, v0, t, y, s.tmp, need != 0, &ro)) return 1;
   const double TdC = s.tmp[S];
   const double yS = y[S];
   const double RuTemp = kRuD * yS;
-  const double multFact = -1.0 / cvc;
-  double T = yS * o.Tref;
-  if (T > 1.0e4) T = 1.0e4;
+  const double multFact = -1.0 / ro.cx;
+  const double T = ro.T, v = o.cp ? ro.v : v0;
+  const double ush = o.cp ? 0.0 : 1.0;
   for (int jj = tid; jj < S; jj += nt) {  // one column per thread, costliest first
     const int j = m.col_order[jj];
     const double t2 = m.mw[j] / clamp_mass_fraction(y[j], o.mmf) * v;
@@ -159,7 +195,7 @@ __device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
       trow += val * s.U[row];
       J[kk] = val * (m.mw[row] * wcol);
     }
-    const double cvj = (nasa_cp(m.thermo + 16 * j, T) - 1.0) * m.ru_inv_mw[j];
+    const double cvj = (nasa_cp(m.thermo + 16 * j, T) - ush) * m.ru_inv_mw[j];
     double tr = trow * RuTemp;
     tr += TdC * cvj * m.mw[j];
     tr *= wcol * multFact;
@@ -171,12 +207,26 @@ __device__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s, doub
   for (int k = tid; k < S; k += nt) s.yp[k] = y[k];
   if (tid == 0) s.yp[S] = ySp;
   __syncthreads();
-  if (rhs_cta(m, o, s, v, s.yp, s.tmp, false, nullptr)) return 1;
+  if (rhs_cta(m, o, s, v0, t, s.yp, s.tmp, false, nullptr)) return 1;
   for (int kk = m.col_ptr[S] + tid; kk < m.col_ptr[S + 1]; kk += nt) {
     const int row = m.row_idx[kk];
     J[kk] = (s.tmp[row] - fy[row]) * mult;
   }
   __syncthreads();
+  if (s.src.esrc != 0.0) {
+    RhsOut r1;
+    if (rhs_cta(m, o, s, v0, t, y, s.yp, false, &r1)) return 1;
+    for (int j = tid; j < S; j += nt) {
+      double cpR, hRT;
+      nasa_cp_h(m.thermo + 16 * j, r1.T, &cpR, &hRT);
+      s.r1d[j] = -((hRT - ush) * (m.ru_inv_mw[j] * r1.T)) / r1.cx;
+    }
+    if (tid == 0) s.r1d[S] = 0.0;
+    const double Tp = r1.T + r1.T * o.sqrt_ur;
+    if (rhs_cta(m, o, s, v0, t, y, s.tmp, false, nullptr, Tp)) return 1;
+    for (int i = tid; i < n; i += nt) s.r1g[i] = (s.tmp[i] - s.yp[i]) / (Tp - r1.T);
+    __syncthreads();
+  }
   return 0;
 }
 
@@ -441,6 +491,15 @@ __device__ void apply_inverse(const Smem &s, int n, int lda, const double *b, do
   __syncthreads();
 }
 
+// Energy-source coupling on a Newton solve x = A^-1 b (Sherman-Morrison):
+// (A - c g d^T)^-1 b = x + w (r1k d.x) with w = A^-1 g, r1k = c / (1 - c d.w).
+__device__ void rank1_fix(const Smem &s, int n, double r1k, double *x) {
+  double a = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) a += s.r1d[i] * x[i];
+  const double dx = block_sum(a, s.red) * r1k;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] += s.r1w[i] * dx;
+  __syncthreads();
+}
 
 __device__ void change_D_cta(double *D, int n, int order, double fac) {
   double R[kMaxOrder + 1][kMaxOrder + 1], U[kMaxOrder + 1][kMaxOrder + 1];
@@ -503,11 +562,15 @@ __device__ void make_consts(Consts &b) {
 // one total), so no thread-0 phase is needed.  Returns 0 when converged, 1
 // when the residual was reduced but not below delta, 2 otherwise.
 template <class LT>
+// Under an energy source the operator and the preconditioner carry the
+// rank-one temperature coupling (r1k as in rank1_fix).
 __device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda,
-                         double delta, const double *b, double *x, int &iters) {
+                         double delta, const double *b, double *x, int &iters, double r1k) {
   const int tid = threadIdx.x, nt = blockDim.x;
+  const bool r1 = s.src.esrc != 0.0;
   double *V = s.V, *u = s.V + (kMaxl + 1) * n, *z = u + n;
   apply_inverse<LT>(s, n, lda, b, z);
+  if (r1) rank1_fix(s, n, r1k, z);
   double a = 0.0;
   for (int i = tid; i < n; i += nt) {
     const double t = z[i] / s.scale[i];
@@ -530,15 +593,22 @@ __device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, doubl
   for (int l = 0; l < kMaxl; ++l) {
     const double *vl = V + l * n;
     double *w = V + (l + 1) * n;
-    for (int i = tid; i < n; i += nt) u[i] = vl[i] * s.scale[i];
+    double du = 0.0;
+    for (int i = tid; i < n; i += nt) {
+      u[i] = vl[i] * s.scale[i];
+      if (r1) du += s.r1d[i] * u[i];
+    }
+    if (r1) du = block_sum(du, s.red);
     __syncthreads();
     for (int i = tid; i < n; i += nt) {  // (I - cJ) u, row i
       double jx = 0.0;
       for (int q = m.jr_ptr[i]; q < m.jr_ptr[i + 1]; ++q) jx += J[m.jr_kk[q]] * u[m.jr_col[q]];
+      if (r1) jx += s.r1g[i] * du;
       s.colk[i] = u[i] - c * jx;
     }
     __syncthreads();
     apply_inverse<LT>(s, n, lda, s.colk, z);
+    if (r1) rank1_fix(s, n, r1k, z);
     for (int i = tid; i < n; i += nt) w[i] = z[i] / s.scale[i];
     for (int k = 0; k <= l; ++k) {  // modified Gram-Schmidt
       const double *vk = V + k * n;
@@ -665,7 +735,7 @@ __device__ void predict_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
 }
 
 template <class LT, int NC>
-__device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
+__device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
                            double *J, double v, double t_end, double rtol, double atol,
                            ReactorStats &st, int lda, double &t_done, double t_off, double T_target,
                            double &t_ign) {
@@ -682,8 +752,17 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   int rc = 0;
   t_done = 0.0;
   double T_prev = s.y[m.nsp] * o.Tref;  // ignition: temperature at the last accepted step
+  double r1k = 0.0;  // energy-source coupling of the current factor
+  auto rank1_setup = [&](double cc) {
+    if (s.src.esrc == 0.0) return;
+    apply_inverse<LT>(s, n, lda, s.r1g, s.r1w);
+    double a = 0.0;
+    for (int i = tid; i < n; i += nt) a += s.r1d[i] * s.r1w[i];
+    const double dw = block_sum(a, s.red);
+    r1k = cc / (1.0 - cc * dw);
+  };
   st.nrhs++;
-  if (rhs_cta(m, o, s, v, s.y, s.f0, false, nullptr)) return -1;
+  if (rhs_cta(m, o, s, v, t_off, s.y, s.f0, false, nullptr)) return -1;
   for (int i = tid; i < n; i += nt) s.scale[i] = atol + fabs(s.y[i]) * rtol;
   __syncthreads();
   const double d0 = vrms(s.y, s.scale), d1 = vrms(s.f0, s.scale);
@@ -693,7 +772,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   __syncthreads();
   double d2 = 0.0;
   st.nrhs++;
-  if (rhs_cta(m, o, s, v, s.tmp, s.f, false, nullptr) == 0) {
+  if (rhs_cta(m, o, s, v, t_off + h0, s.tmp, s.f, false, nullptr) == 0) {
     for (int i = tid; i < n; i += nt) s.d[i] = s.f[i] - s.f0[i];
     __syncthreads();
     d2 = vrms(s.d, s.scale) / h0;
@@ -712,9 +791,10 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
   }
   __syncthreads();
   st.njac++;
-  if (jac_cta(m, o, s, v, s.y, s.f0, J)) { rc = -2; goto failed; }
+  if (jac_cta(m, o, s, v, t_off, s.y, s.f0, J)) { rc = -2; goto failed; }
   st.nlu++;
   if (invert_cta<LT, NC>(m, s, J, c_lu, n, lda)) { rc = -3; goto failed; }
+  rank1_setup(c_lu);
   while (t < t_end) {
     if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
@@ -756,6 +836,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         c_lu = c;
         crate = 1.0;
         if (invert_cta<LT, NC>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
+        rank1_setup(c);
       }
       const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
       bool conv = false;
@@ -763,7 +844,7 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
       double dnorm_old = -1.0;
       for (it = 0; it < kNewtonMaxIter; ++it) {
         st.nrhs++;
-        if (rhs_cta(m, o, s, v, s.y, s.f, false, nullptr)) break;
+        if (rhs_cta(m, o, s, v, t_off + t_new, s.y, s.f, false, nullptr)) break;
         int bad = 0;
         for (int i = tid; i < n; i += nt) bad |= !isfinite(s.f[i]);
         if (__syncthreads_or(bad)) break;
@@ -781,10 +862,11 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
           // Krylov solve can pass the Newton test with a poor correction,
           // and a failure here costs only a Jacobian update or a step cut.
           const double delta = o.eps_lin * o.nlscoef / bc.econ[q] * sqrt((double)n);
-          if (gmres_cta<LT>(m, s, J, c, n, lda, delta, s.tmp, s.yp, st.nkry) != 0) break;
+          if (gmres_cta<LT>(m, s, J, c, n, lda, delta, s.tmp, s.yp, st.nkry, r1k) != 0) break;
           gs = 1.0;  // the Krylov solve uses the current c exactly
         } else {
           apply_inverse<LT>(s, n, lda, s.tmp, s.yp);
+          if (s.src.esrc != 0.0) rank1_fix(s, n, r1k, s.yp);
         }
         double a = 0.0;
         for (int i = tid; i < n; i += nt) {
@@ -815,14 +897,15 @@ __device__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &b
         }
         if (!jac_current) {
           st.nrhs++;
-          if (rhs_cta(m, o, s, v, s.ypred, s.f0, false, nullptr)) { rc = -6; goto failed; }
+          if (rhs_cta(m, o, s, v, t_off + t_new, s.ypred, s.f0, false, nullptr)) { rc = -6; goto failed; }
           st.njac++;
-          if (jac_cta(m, o, s, v, s.ypred, s.f0, J)) { rc = -2; goto failed; }
+          if (jac_cta(m, o, s, v, t_off + t_new, s.ypred, s.f0, J)) { rc = -2; goto failed; }
           jac_current = 1;
           st.nlu++;
           c_lu = c;
           crate = 1.0;
           if (invert_cta<LT, NC>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
+          rank1_setup(c);
           continue;
         }
         change_D_cta(s.D, n, q, 0.5);
@@ -921,7 +1004,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
   const int S = m.nsp, n = S + 1, N = m.nstep, tid = threadIdx.x, nt = blockDim.x;
   Smem s;
   double *p = smem_dyn;
-  double *g = a.rop_scratch + (size_t)blockIdx.x * ((size_t)N + (kMaxOrder + 3) * (size_t)n);
+  double *g = a.rop_scratch + (size_t)blockIdx.x * ((size_t)N + (kMaxOrder + 6) * (size_t)n);
   s.red = p; p += 128;
   s.C = p; p += S;
   s.G = p; p += S;
@@ -931,6 +1014,9 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
   s.Jsm = nullptr;
   if (spill & 4) { s.Jsm = p; p += m.nnz; }
   s.ysrc = nullptr;
+  s.r1g = g + N + (kMaxOrder + 3) * n;
+  s.r1d = s.r1g + n;
+  s.r1w = s.r1d + n;
   s.y = p; p += n;
   s.f = p; p += n;
   s.f0 = p; p += n;
@@ -969,6 +1055,16 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     for (int k = tid; k < S; k += nt) pa += Y0[k] * m.inv_mw[k];
     const double mwmix = 1.0 / block_sum(pa, s.red);
     const double v = 1.0 / (P0 * mwmix / (kRuD * T0));
+    s.src.dpdt = a.dpdt ? a.dpdt[r] : 0.0;
+    s.src.esrc = a.esrc ? a.esrc[r] : 0.0;
+    s.src.P0 = P0;
+    s.src.ysrc = a.ysrc != nullptr;
+    s.src.E0 = 0.0;
+    if (s.src.esrc != 0.0) {  // initial_energy_ (InitializeState)
+      double cx;
+      mix_energy(m, o.cp != 0, false, T0, Y0, false, 0.0, tid, nt,
+                 [&](double x) { return block_sum(x, s.red); }, s.src.E0, cx);
+    }
     for (int k = tid; k < S; k += nt) s.y[k] = Y0[k];
     if (tid == 0) s.y[S] = T0 / o.Tref;
     __syncthreads();
@@ -1003,7 +1099,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
       if (tid == 0) {
         const double Tn = s.y[S] * o.Tref;
         a.T[r] = Tn;
-        a.P[r] = kRuD * Tn / (v * mw2);
+        a.P[r] = end_pressure(o.cp != 0, s.src, a.dt, Tn, mw2, v);
       }
     }
     if (tid == 0) {

@@ -211,6 +211,7 @@ static zrk::SolveOptions options_of(zerork_handle_impl *h) {
   o.threads = I["gpu_threads"];
   o.pred = h->pred;
   o.dT_ign = D["delta_temperature_ignition"];
+  o.constant_pressure = I["constant_volume"] == 0;  // zerork_reactor_manager.cpp:913-917
   return o;
 }
 
@@ -248,19 +249,12 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
     ign = h->own_ign.data();
   }
   const int ns = h->solver->nsp();
-  // pressure-rate and energy sources (reactor_constant_volume_cpu.cpp:87-97)
-  // are not built: refuse non-zero values instead of ignoring them
-  for (int f : {ZERORK_FIELD_DPDT, ZERORK_FIELD_E_SRC})
-    if (const double *x = h->aux[f])
-      for (int r = 0; r < n; ++r)
-        if (x[r] != 0.0) {
-          h->last_error = "non-zero DPDT / E_SRC sources are not supported";
-          std::fprintf(stderr, "zerork_b200: %s\n", h->last_error.c_str());
-          return ZERORK_STATUS_UNKNOWN_ERROR;
-        }
+  // aux sources (zerork_reactor_manager.cpp:1092-1104): DPDT, E_SRC and
+  // Y_SRC per reactor where the caller set them
   int nfail = h->solver->solve(o, n, dt, T, P, mf, ns, cost, gpu, tdel,
                                D["solve_temperature_threshold"], nullptr, &h->last,
-                               h->aux[ZERORK_FIELD_Y_SRC], ign);
+                               h->aux[ZERORK_FIELD_Y_SRC], ign, h->aux[ZERORK_FIELD_DPDT],
+                               h->aux[ZERORK_FIELD_E_SRC]);
   if (nfail < 0) {
     h->last_error = h->solver->last_error;
     std::fprintf(stderr, "zerork_b200: %s\n", h->last_error.c_str());

@@ -52,6 +52,7 @@ ReactorSolver::~ReactorSolver() {
   if (graph_) cudaGraphExecDestroy(graph_);
   cudaFreeHost(hT_); cudaFreeHost(hP_); cudaFreeHost(hY_); cudaFreeHost(horder_); cudaFreeHost(hstats_);
   cudaFreeHost(hsrc_); cudaFreeHost(hign_); cudaFree(dsrc_); cudaFree(dign_);
+  cudaFreeHost(hde_); cudaFree(dde_);
   cudaFree(lu_blob_);
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_); cudaFree(drop_);
@@ -66,7 +67,8 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_);
   cudaFreeHost(hT_); cudaFreeHost(hP_); cudaFreeHost(hY_); cudaFreeHost(horder_); cudaFreeHost(hstats_);
   cudaFreeHost(hsrc_); cudaFreeHost(hign_); cudaFree(dsrc_); cudaFree(dign_);
-  hsrc_ = hign_ = dsrc_ = dign_ = nullptr;
+  cudaFreeHost(hde_); cudaFree(dde_);
+  hsrc_ = hign_ = dsrc_ = dign_ = hde_ = dde_ = nullptr;
   hT_ = hP_ = hY_ = nullptr;
   horder_ = nullptr;
   hstats_ = nullptr;
@@ -102,6 +104,8 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   if ((e = cudaMallocHost(&hign_, cap * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&dsrc_, cap * S * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&dign_, cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hde_, 2 * (size_t)cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dde_, 2 * (size_t)cap * sizeof(double))) != cudaSuccess) return e;
   cap_ = cap;
   cap_fp32_ = fp32;
   return cudaSuccess;
@@ -110,7 +114,8 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
 int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
                          int stride, double *cost, double *gpu_time, double *temp_delta,
                          double temp_threshold, std::vector<ReactorStats> *stats,
-                         SolveStatsTotals *tot, const double *ysrc, double *t_ign) {
+                         SolveStatsTotals *tot, const double *ysrc, double *t_ign,
+                         const double *dpdt, const double *esrc) {
   if (n <= 0) return 0;
   const int S = tables_.nsp;
   cudaError_t e = reserve(n, o.lu_fp32);
@@ -207,6 +212,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.lim = o.lim;
   io.sqrt_ur = std::sqrt(2.2204460492503131e-16);
   io.lu_fp32 = o.lu_fp32 ? 1 : 0;
+  io.cp = o.constant_pressure ? 1 : 0;
   IntegArgs a;
   std::memset(&a, 0, sizeof(a));
   a.n_reactors = n;
@@ -225,9 +231,13 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   a.rop_scratch = drop_;
   a.ysrc = ysrc ? dsrc_ : nullptr;
   a.t_ign = (t_ign && o.dT_ign > 0.0) ? dign_ : nullptr;
+  a.dpdt = dpdt ? dde_ : nullptr;
+  a.esrc = esrc ? dde_ + cap_ : nullptr;
   cudaStream_t s = stream_;
   std::memcpy(horder_, order.data(), n * sizeof(int));
   if (ysrc) std::memcpy(hsrc_, ysrc, (size_t)n * S * sizeof(double));
+  if (dpdt) std::memcpy(hde_, dpdt, n * sizeof(double));
+  if (esrc) std::memcpy(hde_ + cap_, esrc, n * sizeof(double));
   if (method == 1) {
     a.state = dstate_;
     a.state_stride = m.nnz;
@@ -260,6 +270,9 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     q(cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
     q(cudaMemcpyAsync(dorder_, horder_, n * sizeof(int), cudaMemcpyHostToDevice, s));
     if (a.ysrc) q(cudaMemcpyAsync(dsrc_, hsrc_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (a.dpdt) q(cudaMemcpyAsync(dde_, hde_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (a.esrc)
+      q(cudaMemcpyAsync(dde_ + cap_, hde_ + cap_, n * sizeof(double), cudaMemcpyHostToDevice, s));
     q(cudaMemsetAsync(dhead_, 0, sizeof(int), s));
     q(cudaEventRecordWithFlags(ev0_, s, cudaEventRecordExternal));  // a timing node in the graph
     q(method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)

@@ -3,8 +3,10 @@
 // Mirrors what ZeroRKReactorManager::SolveReactors does per call
 // (applications/cfd_plugin/zerork_reactor_manager.cpp:835-1155): order the
 // reactors by the previous call's cost (sort_reactors), integrate every
-// reactor for dt, write back T, P, mass fractions, cost (steps), time and
-// temperature delta.  All reactors run on the GPU (no CPU fallback).
+// reactor (constant volume or constant pressure, with optional DPDT, E_SRC
+// and Y_SRC sources) for dt, write back T, P, mass fractions, cost (steps),
+// time and temperature delta.  All reactors run on the GPU (no CPU
+// fallback).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -33,6 +35,7 @@ struct SolveOptions {
   int threads = 0;        // CTA size of the dense method (0 = automatic)
   PredDev pred{};         // learned predictor (dense method only)
   double dT_ign = 0.0;    // delta_temperature_ignition (> 0: record ignition times)
+  bool constant_pressure = false;  // plugin option constant_volume = 0
 };
 
 struct SolveStatsTotals {
@@ -53,11 +56,13 @@ class ReactorSolver {
   // cost/gpu_time/temp_delta may be null.  Returns the number of failed
   // reactors (state left unchanged for those), or -1 on a CUDA error.
   // ysrc: optional mass-fraction sources [n][nsp] (1/s); t_ign: optional
-  // ignition times [n] (written when o.dT_ign > 0, -1 where not reached).
+  // ignition times [n] (written when o.dT_ign > 0, -1 where not reached);
+  // dpdt, esrc: optional pressure rates (Pa/s) and energy sources (J/kg/s) [n].
   int solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
             int stride, double *cost, double *gpu_time, double *temp_delta,
             double temp_threshold, std::vector<ReactorStats> *stats, SolveStatsTotals *tot,
-            const double *ysrc = nullptr, double *t_ign = nullptr);
+            const double *ysrc = nullptr, double *t_ign = nullptr, const double *dpdt = nullptr,
+            const double *esrc = nullptr);
   std::string last_error;
 
  private:
@@ -82,6 +87,7 @@ class ReactorSolver {
   // pinned host staging (fixed addresses for the captured copies)
   double *hT_ = nullptr, *hP_ = nullptr, *hY_ = nullptr, *hsrc_ = nullptr, *hign_ = nullptr;
   double *dsrc_ = nullptr, *dign_ = nullptr;
+  double *hde_ = nullptr, *dde_ = nullptr;  // [dpdt | esrc], cap_ each
   int *horder_ = nullptr;
   ReactorStats *hstats_ = nullptr;
   // one CUDA graph per call configuration: H2D copies, queue reset, the
