@@ -40,13 +40,16 @@ def _compile(src, verbose=False):
                glob.glob(os.path.join(HERE, "..", "include", "*.h")))
     newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in headers])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
-        return obj, ""
+        return obj, None
     cmd = [nvcc(), "-c", src, "-o", obj] + _flags(src)
     if verbose and src.endswith(".cu"):
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    # date the object by the inputs it was compiled from, so that a source
+    # edited while the compiler ran counts as newer on the next build
+    os.utime(obj, (newest, newest))
     return obj, r.stderr
 
 
@@ -61,7 +64,8 @@ def build(verbose=False):
         for _, log in res:
             if log:
                 print(log)
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+    compiled = any(log is not None for _, log in res)
+    if compiled or not os.path.exists(LIB):
         cmd = [nvcc(), "-shared", "-o", LIB] + ARCH + objs + ["-lcudart_static", "-ldl", "-lrt", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

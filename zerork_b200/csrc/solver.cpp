@@ -179,7 +179,8 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     per_sm = std::max(1, std::min(per_sm, 65536 / (dthreads * 128)));
     dctas = std::min(n, sms * per_sm);
   }
-  if (!rop_smem || (method == 1 && spill > 0)) {
+  // the dense integrator's slice also holds the energy-source coupling vectors
+  if (!rop_smem || method == 1) {
     size_t need = method == 1 ? (size_t)dctas * dense_spill_doubles(m) * sizeof(double)
                               : (size_t)ctas * W * m.nstep * sizeof(double);
     if (need > drop_bytes_) {
