@@ -389,7 +389,7 @@ failed:
 
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
                      const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
-                     const double *y_src, double dpdt, double e_src, double *t_ign,
+                     const double *y_src, double dpdt, double e_src, int fix_T, double *t_ign,
                      zo_bdf_stats *st) {
   bdf_t b;
   memset(&b, 0, sizeof(b));
@@ -420,6 +420,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   b.r1d = b.r1g + n;
   double *y = (double *)calloc(n, sizeof(double));
   b.r->cp = o->constant_volume == 0;
+  b.r->fix_T = fix_T;
   zo_reactor_init_state(b.r, *T, *P, Y, dpdt, e_src, y_src);
   b.t_ign = t_ign;
   if (t_ign) *t_ign = -1.0;
@@ -448,8 +449,8 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   free(ystart);
   b.st.status = rc;
   if (rc == 0) {
-    *T = y[ns] * o->Tref;
     for (int j = 0; j < ns; ++j) Y[j] = y[j];
+    *T = zo_reactor_end_temperature(b.r, dt, Y, y[ns] * o->Tref);
     *P = zo_reactor_pressure(b.r, dt, *T, Y);
   }
   if (st) *st = b.st;
@@ -461,7 +462,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
 int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
                            int nthreads, int n, double dt, double *T, double *P, double *Y,
                            const double *y_src, const double *dpdt, const double *e_src,
-                           double *t_ign, zo_bdf_stats *stats) {
+                           const int *fix_T, double *t_ign, zo_bdf_stats *stats) {
   int nfail = 0;
   if (nthreads < 1) nthreads = 1;
 #pragma omp parallel for num_threads(nthreads) schedule(dynamic, 1) reduction(+ : nfail)
@@ -471,7 +472,8 @@ int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo
     zo_bdf_stats st;
     if (zo_reactor_solve(t, p, &kin, o, dt, &T[r], &P[r], &Y[(size_t)r * t->nsp],
                          y_src ? &y_src[(size_t)r * t->nsp] : NULL, dpdt ? dpdt[r] : 0.0,
-                         e_src ? e_src[r] : 0.0, t_ign ? &t_ign[r] : NULL, &st))
+                         e_src ? e_src[r] : 0.0, fix_T ? fix_T[r] : 0, t_ign ? &t_ign[r] : NULL,
+                         &st))
       ++nfail;
     if (stats) stats[r] = st;
   }

@@ -407,6 +407,13 @@ void zo_reactor_init_state(zo_reactor *r, double T, double P, const double *Y, d
   r->y_src = y_src;
 }
 
+double zo_reactor_end_temperature(const zo_reactor *r, double t, const double *Y, double T_state) {
+  if (!r->fix_T) return T_state;
+  const double E = r->E0 + r->e_src * t;
+  return r->cp ? r->kin.temp_from_HY(r->kin.ctx, E, Y, r->T0)
+               : r->kin.temp_from_EY(r->kin.ctx, E, Y, r->T0);
+}
+
 double zo_reactor_pressure(const zo_reactor *r, double t, double T, const double *Y) {
   if (r->cp && !r->y_src) return r->P0 + r->dpdt * t;
   const double P = r->kin.pressure_TVY(r->kin.ctx, T, r->inv_density, Y);
@@ -421,7 +428,7 @@ double zo_reactor_pressure(const zo_reactor *r, double t, double T, const double
 int zo_reactor_rhs(zo_reactor *r, const double *y, double *ydot) {
   const int n = r->nsp;
   const double dt = r->time;
-  double T = y[n] * r->Tref;
+  double T = r->fix_T ? r->T0 : y[n] * r->Tref;
   if (T <= 0.0) return 1;
   if (T > 1.0e4) T = 1.0e4;
   double v = r->inv_density;
@@ -461,7 +468,7 @@ int zo_reactor_rhs(zo_reactor *r, const double *y, double *ydot) {
     }
   }
   double dT_dt = -esum * ZO_RU * y[n] / r->mean_cv;
-  ydot[n] = dT_dt + (r->e_src + r->dpdt * v) / (r->mean_cv * r->Tref);
+  ydot[n] = r->fix_T ? 0.0 : dT_dt + (r->e_src + r->dpdt * v) / (r->mean_cv * r->Tref);
   double es = 0.0;
   for (int j = 0; j < n; ++j) {
     double m = fabs(r->cre[j]) + fabs(r->des[j]);
@@ -634,6 +641,7 @@ int zo_jac_values(zo_reactor *r, const zo_jac_pattern *p, const double *y, const
     int lr = p->last_row[j];
     jac[lr] *= (1.0 / mw[j]) * multFact;
     if (scale) scale[lr] *= fabs((1.0 / mw[j]) * multFact);
+    if (r->fix_T) jac[lr] = 0.0; /* no temperature row without solve_temperature_ */
   }
   /* d(ydot)/dT by forward difference */
   double dT = y[ns] * sqrt_ur;

@@ -123,6 +123,9 @@ typedef struct zo_reactor {
   double T_force;  /* > 0: evaluate at this temperature instead of the state's or the
                       energy source's (a finite-difference hook of the integrator) */
   double T_used;   /* temperature the last evaluation used */
+  int fix_T;       /* 1: temperature not solved (solve_temperature_ false,
+                      zerork_reactor_manager.cpp:1107-1113): the rates see T0
+                      (or the energy source's temperature), Tdot = 0 */
   double *lim, *C, *net, *cre, *des, *rop, *u_RT, *cv_spc, mean_cv;
   double *tmp1, *tmp2, *tmp3;
   double *yscale;  /* [nsp+1] rounding scale of the last ydot: sum of |terms| */
@@ -143,6 +146,10 @@ void zo_reactor_init_state(zo_reactor *r, double T, double P, const double *Y, d
 /* GetState's pressure at time t for the end state (T, Y)
  * (reactor_constant_volume_cpu.cpp:59, reactor_constant_pressure_cpu.cpp:59-63). */
 double zo_reactor_pressure(const zo_reactor *r, double t, double T, const double *Y);
+/* GetState's temperature at time t: the state's T_state, or with fix_T the
+ * temperature of the energy E0 + e_src t at composition Y
+ * (reactor_constant_volume_cpu.cpp:51-56, reactor_constant_pressure_cpu.cpp:52-57). */
+double zo_reactor_end_temperature(const zo_reactor *r, double t, const double *Y, double T_state);
 
 /* ydot for y = [Y, T/Tref] at time r->time: GetTimeDerivative of
  * reactor_constant_volume_cpu.cpp:64-128 or reactor_constant_pressure_cpu.cpp:

@@ -124,7 +124,7 @@ def _bind_common(lib):
         lib.zo_reactor_solve_batch.argtypes = [C.POINTER(ZoTables), C.POINTER(ZoJacPattern),
                                                C.POINTER(ZoBdfOpts), C.c_int, C.c_int, C.c_double,
                                                _dp, _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
-                                               C.c_void_p, C.c_void_p]
+                                               C.c_void_p, C.c_void_p, C.c_void_p]
         lib.zo_reactor_solve_batch.restype = C.c_int
     return lib
 
@@ -325,11 +325,13 @@ class OracleTables:
         return _reactor_rhs(lambda *a: self.lib.zo_reactor_rhs_batch(self.ptr, C.byref(k), *a),
                             self.nsp, cp, T0, P0, Y0, tm, y, dpdt, e_src, y_src)
 
-    def solve(self, T, P, Y, dt, nthreads=1, y_src=None, dpdt=None, e_src=None, **opts):
+    def solve(self, T, P, Y, dt, nthreads=1, y_src=None, dpdt=None, e_src=None, fix_T=None,
+              **opts):
         """Oracle BDF integration of reactors (reactor-major Y), constant
         volume unless opts sets constant_volume=0.  y_src: optional [n, nsp]
         mass-fraction source terms; dpdt, e_src: optional [n] pressure-rate
-        (Pa/s) and energy (J/kg/s) sources.  Returns (T, P, Y,
+        (Pa/s) and energy (J/kg/s) sources; fix_T: optional [n] flags of
+        reactors integrated without solving the temperature.  Returns (T, P, Y,
         stats-dict-of-arrays); stats["t_ign"] holds the ignition times when
         opts sets dT_ign > 0 (-1 where not reached).  opts override the
         plugin defaults."""
@@ -344,9 +346,10 @@ class OracleTables:
         st = (ZoBdfStats * n)()
         ys, dp, es = (None if a is None else np.ascontiguousarray(a, dtype=np.float64)
                       for a in (y_src, dpdt, e_src))
+        fx = None if fix_T is None else np.ascontiguousarray(fix_T, dtype=np.int32)
         tign = np.full(n, -1.0)
         self.lib.zo_reactor_solve_batch(self.ptr, self.pat, C.byref(o), nthreads, n, float(dt),
-                                        T, P, Y, _vp(ys), _vp(dp), _vp(es),
+                                        T, P, Y, _vp(ys), _vp(dp), _vp(es), _vp(fx),
                                         tign.ctypes.data, C.cast(st, C.c_void_p))
         stats = {f: np.array([getattr(st[i], f) for i in range(n)]) for f, _ in ZoBdfStats._fields_}
         stats["t_ign"] = tign

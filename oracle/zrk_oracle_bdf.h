@@ -57,11 +57,13 @@ void zo_bdf_default_opts(zo_bdf_opts *o);
  * Integrate / GetState of the cfd_plugin (reactor_constant_volume_cpu.cpp:
  * 15-61, reactor_constant_pressure_cpu.cpp:15-66, zerork_reactor_manager.cpp:
  * 1090-1146), with optional mass-fraction sources y_src [nsp] (or NULL), a
- * pressure rate dpdt (Pa/s) and an energy source e_src (J/kg/s).  On return
- * T, P, Y hold the end state. */
+ * pressure rate dpdt (Pa/s) and an energy source e_src (J/kg/s).  fix_T = 1
+ * integrates without solving the temperature (the plugin's
+ * always_solve_temperature = 0 for a reactor whose previous temperature
+ * delta is not positive).  On return T, P, Y hold the end state. */
 int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinetics *kin,
                      const zo_bdf_opts *o, double dt, double *T, double *P, double *Y,
-                     const double *y_src, double dpdt, double e_src, double *t_ign,
+                     const double *y_src, double dpdt, double e_src, int fix_T, double *t_ign,
                      zo_bdf_stats *st);
 
 /* Batch over reactors (reactor-major Y [n][nsp]) with nthreads OpenMP
@@ -69,7 +71,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
 int zo_reactor_solve_batch(const zo_tables *t, const zo_jac_pattern *p, const zo_bdf_opts *o,
                            int nthreads, int n, double dt, double *T, double *P, double *Y,
                            const double *y_src, const double *dpdt, const double *e_src,
-                           double *t_ign, zo_bdf_stats *stats);
+                           const int *fix_T, double *t_ign, zo_bdf_stats *stats);
 
 #ifdef __cplusplus
 }

@@ -225,6 +225,54 @@ def test_pressure_energy_sources_and_constant_pressure(gpu, cv, method, fp32, ys
     assert np.all(np.sign(Tg - Tn)[big] == np.sign(esrc)[big])
 
 
+@pytest.mark.parametrize("cv,method", [(1, 1), (0, 1), (1, 2)])
+def test_fixed_temperature_reactors(gpu, cv, method, mech_dir):
+    """always_solve_temperature = 0: reactors whose input TEMPERATURE_DELTA is
+    not positive integrate at their initial temperature and report the
+    temperature of their energy at the end composition; the others solve the
+    temperature (zerork_reactor_manager.cpp:1107-1113,
+    reactor_constant_volume_cpu.cpp:51-56).  Against the oracle with the same
+    per-reactor choice."""
+    from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    pm = zb.Mechanism(mf, tf, device=False)
+    from zerork_b200 import mechgen
+    n, dt = 16, 1e-3
+    T, P, Y = mechgen.reactor_states(g, n, "c1", seed=31)
+    tdel_in = np.where(np.arange(n) % 2 == 0, 0.0, 50.0)
+    esrc = np.where(np.arange(n) % 4 == 0, 3e7, 0.0)
+    p = Plugin(mf, tf, constant_volume=cv, gpu_method=method, always_solve_temperature=0)
+    tdel = p.set_aux_field("TEMPERATURE_DELTA", tdel_in.copy())
+    p.set_aux_field("E_SRC", esrc)
+    Tg, Pg, Yg = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert p.solve(dt, Tg, Pg, Yg) == 0
+    ot = oracle_tables(pm)
+    nt = os.cpu_count() or 1
+    fix = (tdel_in <= 0).astype(np.int32)
+    src = dict(e_src=esrc, fix_T=fix, constant_volume=cv)
+    To, Po, Yo, so = ot.solve(T, P, Y, dt, nthreads=nt, **src)
+    Tt, Pt, Yt, st = ot.solve(T, P, Y, dt, nthreads=nt, rtol=1e-10, atol=1e-22, max_steps=400000,
+                              **src)
+    ok = (so["status"] == 0) & (st["status"] == 0)
+    assert ok.sum() >= n - 2
+    for g_, o_, t_, rel in ((Tg, To, Tt, 1e-5), (Pg, Po, Pt, 1e-8)):
+        eo, eg = np.abs(o_ - t_)[ok], np.abs(g_ - t_)[ok]
+        assert np.all(eg <= 50 * np.maximum(eo, 10 * np.median(eo)) + rel * np.abs(t_[ok])), (eg, eo)
+    eo_Y, eg_Y = np.max(np.abs(Yo - Yt), axis=1)[ok], np.max(np.abs(Yg - Yt), axis=1)[ok]
+    assert np.all(eg_Y <= 50 * np.maximum(eo_Y, 10 * np.median(eo_Y)) + 1e-8)
+    # the fixed-temperature reactors differ from a run that solves every
+    # temperature, and the output deltas feed the next call's choice
+    q = Plugin(mf, tf, constant_volume=cv, gpu_method=method)
+    q.set_aux_field("E_SRC", esrc)
+    Ta, Pa, Ya = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert q.solve(dt, Ta, Pa, Ya) == 0
+    assert np.all(np.abs(Ya - Yg).max(axis=1)[fix == 0] < 1e-6)
+    assert np.any(np.abs(Ya - Yg).max(axis=1)[fix == 1] > 1e-6)
+    d = Tg - T
+    assert np.allclose(tdel, np.where(d < 2.0, 0.0, d))
+
+
 def test_constant_pressure_c3_subset(gpu, mech_dir):
     """Constant-pressure C3 reactors (160 species, dense integrator) without
     sources: end state against the oracle, pressure unchanged."""

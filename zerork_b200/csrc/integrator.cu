@@ -70,7 +70,7 @@ __device__ __forceinline__ int rhs_warp(const DevMech &m, const IntegOpts &o, co
                                         double T_force = 0.0) {
   const int S = m.nsp;
   const double yS = y[S];
-  double T = yS * o.Tref;
+  double T = w.src.fixT ? w.src.T0 : yS * o.Tref;
   if (!(T > 0.0)) return 1;
   if (T > 1.0e4) T = 1.0e4;
   double v = v0;
@@ -114,7 +114,8 @@ __device__ __forceinline__ int rhs_warp(const DevMech &m, const IntegOpts &o, co
     }
   }
   const double es = wsum(pe);
-  if (lane == 0) ydot[S] = -es * kRuD * yS / cv + (w.src.esrc + w.src.dpdt * v) / (cv * o.Tref);
+  if (lane == 0)
+    ydot[S] = w.src.fixT ? 0.0 : -es * kRuD * yS / cv + (w.src.esrc + w.src.dpdt * v) / (cv * o.Tref);
   if (out) *out = RhsOut{cv, T, v};
   __syncwarp();
   return 0;
@@ -161,7 +162,7 @@ __device__ int jac_warp(const DevMech &m, const IntegOpts &o, const Warp &w, dou
       double tr = trow * RuTemp;
       tr += TdC * cvj * m.mw[j];
       tr *= wcol * multFact;
-      J[k1] = tr;
+      J[k1] = w.src.fixT ? 0.0 : tr;  // no temperature row when T is not solved
     }
   }
   __syncwarp();
@@ -751,8 +752,10 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     w.src.esrc = a.esrc ? a.esrc[r] : 0.0;
     w.src.P0 = P0;
     w.src.ysrc = a.ysrc != nullptr;
+    w.src.fixT = !o.always_T && a.tdel_in && !(a.tdel_in[r] > 0.0);
+    w.src.T0 = T0;
     w.src.E0 = 0.0;
-    if (w.src.esrc != 0.0) {  // initial_energy_ (InitializeState)
+    if (w.src.esrc != 0.0 || w.src.fixT) {  // initial_energy_ (InitializeState)
       double cx;
       mix_energy(m, o.cp != 0, false, T0, Y0, false, 0.0, lane, 32,
                  [](double x) { return wsum(x); }, w.src.E0, cx);
@@ -787,8 +790,9 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
         a.Y[(size_t)r * S + s] = ys;
         pb += ys * m.inv_mw[s];
       }
-      const double Tn = V.y[S] * o.Tref;
       const double mw2 = 1.0 / wsum(pb);
+      const double Tn = end_temperature(m, o.cp != 0, w.src, a.dt, V.y, V.y[S] * o.Tref, lane, 32,
+                                        [](double x) { return wsum(x); });
       if (lane == 0) {
         a.T[r] = Tn;
         a.P[r] = end_pressure(o.cp != 0, w.src, a.dt, Tn, mw2, v);

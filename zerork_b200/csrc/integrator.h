@@ -46,6 +46,8 @@ struct IntegOpts {
   double Tref, mmf, lim, sqrt_ur;
   int lu_fp32;  // factor and apply the Newton matrix in FP32
   int cp;       // 1: constant-pressure reactor (plugin option constant_volume = 0)
+  int always_T; // always_solve_temperature: 0 = integrate at fixed temperature the
+                // reactors whose input temperature delta is <= 0
   double eps_lin;  // Krylov tolerance: eps_lin * nlscoef / error constant (WRMS)
   PredDev pred;    // learned predictor (dense integrator only; enabled = 0: off)
   double dT_ign;   // delta_temperature_ignition: > 0 records when T reaches T0 + dT_ign
@@ -75,6 +77,7 @@ struct IntegArgs {
   double *t_ign;            // optional ignition times [n_reactors] (-1: not reached)
   const double *dpdt;       // optional pressure rates [n_reactors] (Pa/s)
   const double *esrc;       // optional energy sources [n_reactors] (J/kg/s)
+  const double *tdel_in;    // previous temperature deltas [n_reactors] (read when !always_T)
 };
 
 size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);

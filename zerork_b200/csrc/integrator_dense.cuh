@@ -103,7 +103,7 @@ __device__ __forceinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, con
                                        bool clamp, RhsOut *out, double T_force = 0.0) {
   const int S = m.nsp, tid = threadIdx.x, nt = blockDim.x;
   const double yS = y[S];
-  double T = yS * o.Tref;
+  double T = s.src.fixT ? s.src.T0 : yS * o.Tref;
   if (!(T > 0.0)) return 1;
   if (T > 1.0e4) T = 1.0e4;
   double v = v0;
@@ -152,7 +152,8 @@ __device__ __forceinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, con
     }
   }
   const double es = block_sum(pe, s.red);
-  if (tid == 0) ydot[S] = -es * kRuD * yS / cv + (s.src.esrc + s.src.dpdt * v) / (cv * o.Tref);
+  if (tid == 0)
+    ydot[S] = s.src.fixT ? 0.0 : -es * kRuD * yS / cv + (s.src.esrc + s.src.dpdt * v) / (cv * o.Tref);
   if (out) *out = RhsOut{cv, T, v};
   __syncthreads();
   return 0;
@@ -199,7 +200,7 @@ __device__ __forceinline__ int jac_cta(const DevMech &m, const IntegOpts &o, con
     double tr = trow * RuTemp;
     tr += TdC * cvj * m.mw[j];
     tr *= wcol * multFact;
-    J[k1] = tr;
+    J[k1] = s.src.fixT ? 0.0 : tr;  // no temperature row when T is not solved
   }
   __syncthreads();
   const double ySp = yS + yS * o.sqrt_ur;
@@ -1059,8 +1060,10 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     s.src.esrc = a.esrc ? a.esrc[r] : 0.0;
     s.src.P0 = P0;
     s.src.ysrc = a.ysrc != nullptr;
+    s.src.fixT = !o.always_T && a.tdel_in && !(a.tdel_in[r] > 0.0);
+    s.src.T0 = T0;
     s.src.E0 = 0.0;
-    if (s.src.esrc != 0.0) {  // initial_energy_ (InitializeState)
+    if (s.src.esrc != 0.0 || s.src.fixT) {  // initial_energy_ (InitializeState)
       double cx;
       mix_energy(m, o.cp != 0, false, T0, Y0, false, 0.0, tid, nt,
                  [&](double x) { return block_sum(x, s.red); }, s.src.E0, cx);
@@ -1096,8 +1099,9 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
         pb += ys * m.inv_mw[k];
       }
       const double mw2 = 1.0 / block_sum(pb, s.red);
+      const double Tn = end_temperature(m, o.cp != 0, s.src, a.dt, s.y, s.y[S] * o.Tref, tid, nt,
+                                        [&](double x) { return block_sum(x, s.red); });
       if (tid == 0) {
-        const double Tn = s.y[S] * o.Tref;
         a.T[r] = Tn;
         a.P[r] = end_pressure(o.cp != 0, s.src, a.dt, Tn, mw2, v);
       }

@@ -212,6 +212,7 @@ static zrk::SolveOptions options_of(zerork_handle_impl *h) {
   o.pred = h->pred;
   o.dT_ign = D["delta_temperature_ignition"];
   o.constant_pressure = I["constant_volume"] == 0;  // zerork_reactor_manager.cpp:913-917
+  o.always_solve_T = I["always_solve_temperature"] != 0;  // :1107-1113
   return o;
 }
 

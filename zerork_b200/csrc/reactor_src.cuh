@@ -24,8 +24,14 @@ struct ReactorSrc {
   double P0 = 0.0;    // pressure at the start of the call
   double E0 = 0.0;    // mass internal energy (constant volume) or enthalpy
                       // (constant pressure) at the start; set when esrc != 0
+                      // or fixT
   bool ysrc = false;  // mass-fraction sources present: the constant-pressure
                       // reactor then keeps its initial density
+  bool fixT = false;  // temperature not solved (always_solve_temperature = 0
+                      // and a previous temperature delta <= 0,
+                      // zerork_reactor_manager.cpp:1107-1113): the rates see
+                      // T0 (or the energy source's temperature), Tdot = 0
+  double T0 = 0.0;    // temperature at the start of the call
 };
 
 // NASA-7 c_p/R and h/RT, the arithmetic of nasa_cp_h_g without g.
@@ -138,6 +144,17 @@ __device__ void source_T_v(const DevMech &m, bool cp, const ReactorSrc &src, dou
       v = 1.0 / (P * mw / (kRuD * T));
     }
   }
+}
+
+// GetState's temperature at the end time t_end for the end composition y:
+// the state's T_state, or, when the temperature was not solved, the
+// temperature of the energy E0 + esrc t_end (reactor_constant_volume_cpu.cpp:
+// 51-56, reactor_constant_pressure_cpu.cpp:52-57).
+template <class Red>
+__device__ double end_temperature(const DevMech &m, bool cp, const ReactorSrc &src, double t_end,
+                                  const double *y, double T_state, int i0, int stride, Red red) {
+  if (!src.fixT) return T_state;
+  return temp_from_energy(m, cp, src.E0 + src.esrc * t_end, y, false, 0.0, src.T0, i0, stride, red);
 }
 
 // GetState's pressure at the end time t_end for the end state (T, mixture

@@ -104,8 +104,8 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   if ((e = cudaMallocHost(&hign_, cap * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&dsrc_, cap * S * sizeof(double))) != cudaSuccess) return e;
   if ((e = cudaMalloc(&dign_, cap * sizeof(double))) != cudaSuccess) return e;
-  if ((e = cudaMallocHost(&hde_, 2 * (size_t)cap * sizeof(double))) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&dde_, 2 * (size_t)cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMallocHost(&hde_, 3 * (size_t)cap * sizeof(double))) != cudaSuccess) return e;
+  if ((e = cudaMalloc(&dde_, 3 * (size_t)cap * sizeof(double))) != cudaSuccess) return e;
   cap_ = cap;
   cap_fp32_ = fp32;
   return cudaSuccess;
@@ -214,6 +214,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.sqrt_ur = std::sqrt(2.2204460492503131e-16);
   io.lu_fp32 = o.lu_fp32 ? 1 : 0;
   io.cp = o.constant_pressure ? 1 : 0;
+  io.always_T = o.always_solve_T ? 1 : 0;
   IntegArgs a;
   std::memset(&a, 0, sizeof(a));
   a.n_reactors = n;
@@ -234,11 +235,13 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   a.t_ign = (t_ign && o.dT_ign > 0.0) ? dign_ : nullptr;
   a.dpdt = dpdt ? dde_ : nullptr;
   a.esrc = esrc ? dde_ + cap_ : nullptr;
+  a.tdel_in = (!o.always_solve_T && temp_delta) ? dde_ + 2 * cap_ : nullptr;
   cudaStream_t s = stream_;
   std::memcpy(horder_, order.data(), n * sizeof(int));
   if (ysrc) std::memcpy(hsrc_, ysrc, (size_t)n * S * sizeof(double));
   if (dpdt) std::memcpy(hde_, dpdt, n * sizeof(double));
   if (esrc) std::memcpy(hde_ + cap_, esrc, n * sizeof(double));
+  if (a.tdel_in) std::memcpy(hde_ + 2 * cap_, temp_delta, n * sizeof(double));
   if (method == 1) {
     a.state = dstate_;
     a.state_stride = m.nnz;
@@ -274,6 +277,9 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     if (a.dpdt) q(cudaMemcpyAsync(dde_, hde_, n * sizeof(double), cudaMemcpyHostToDevice, s));
     if (a.esrc)
       q(cudaMemcpyAsync(dde_ + cap_, hde_ + cap_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (a.tdel_in)
+      q(cudaMemcpyAsync(dde_ + 2 * cap_, hde_ + 2 * cap_, n * sizeof(double),
+                        cudaMemcpyHostToDevice, s));
     q(cudaMemsetAsync(dhead_, 0, sizeof(int), s));
     q(cudaEventRecordWithFlags(ev0_, s, cudaEventRecordExternal));  // a timing node in the graph
     q(method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)

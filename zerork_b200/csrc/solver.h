@@ -36,6 +36,8 @@ struct SolveOptions {
   PredDev pred{};         // learned predictor (dense method only)
   double dT_ign = 0.0;    // delta_temperature_ignition (> 0: record ignition times)
   bool constant_pressure = false;  // plugin option constant_volume = 0
+  bool always_solve_T = true;      // always_solve_temperature; false: reactors whose
+                                   // input temperature delta is <= 0 keep T fixed
 };
 
 struct SolveStatsTotals {
@@ -87,7 +89,7 @@ class ReactorSolver {
   // pinned host staging (fixed addresses for the captured copies)
   double *hT_ = nullptr, *hP_ = nullptr, *hY_ = nullptr, *hsrc_ = nullptr, *hign_ = nullptr;
   double *dsrc_ = nullptr, *dign_ = nullptr;
-  double *hde_ = nullptr, *dde_ = nullptr;  // [dpdt | esrc], cap_ each
+  double *hde_ = nullptr, *dde_ = nullptr;  // [dpdt | esrc | temp_delta in], cap_ each
   int *horder_ = nullptr;
   ReactorStats *hstats_ = nullptr;
   // one CUDA graph per call configuration: H2D copies, queue reset, the
