@@ -229,9 +229,9 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
             m = min(n_reactors, 2 * nth)
             t0 = time.perf_counter()
             To, Po, Yo, so = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth)
-            dt = time.perf_counter() - t0
+            elapsed = time.perf_counter() - t0
             ok = so["status"] == 0
-            out["cpu_oracle"] = {"value": m / dt, "unit": "reactors/s", "cores": nth, "kind": "port",
+            out["cpu_oracle"] = {"value": m / elapsed, "unit": "reactors/s", "cores": nth, "kind": "port",
                                  "sample": f"first {m} of the {n_reactors} reactors, restated "
                                            "BDF/Newton with dense LU (FP64), one reactor per thread",
                                  "failed": int((~ok).sum())}
