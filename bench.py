@@ -63,7 +63,7 @@ class Clocks:
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu):
-        self.gpu, self.rows, self.proc = gpu, [], None
+        self.gpu, self.rows, self.proc, self.start = gpu, [], None, 0
 
     def __enter__(self):
         try:
@@ -73,6 +73,12 @@ class Clocks:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a while to start: wait (bounded) for its first
+            # row and keep only the rows from the region itself
+            deadline = time.time() + 5.0
+            while not self.rows and time.time() < deadline:
+                time.sleep(0.01)
+            self.start = len(self.rows)
         except Exception:
             self.proc = None
         return self
@@ -83,6 +89,10 @@ class Clocks:
 
     def __exit__(self, *a):
         if self.proc:
+            # a short region may end between two samples: take the next one
+            deadline = time.time() + 1.0
+            while len(self.rows) <= self.start and time.time() < deadline:
+                time.sleep(0.01)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -90,14 +100,15 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        rows = self.rows[self.start:]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4)
+        reasons = sorted({names[i] for r in rows for i in range(4)
                           if len(r) > 3 + i and r[3 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+                "samples": len(rows)}
 
 
 def peaks():
