@@ -22,6 +22,11 @@ def test_defaults_match_reference_manager():
     assert p.get_double("min_mass_fraction") == 1.0e-30
     assert p.get_int("sort_reactors") == 1
     assert p.get_string("mech_filename") == "mech.dat"
+    # reactor model: constant volume, temperature always solved
+    assert p.get_int("constant_volume") == 1
+    assert p.get_int("always_solve_temperature") == 1
+    assert p.get_double("solve_temperature_threshold") == 2.0
+    assert p.get_double("delta_temperature_ignition") == 0.0
 
 
 def test_option_roundtrip_and_unknown():
@@ -46,6 +51,12 @@ def test_options_file(tmp_path):
     assert p.get_int("max_steps") == 3000
     assert p.get_string("reactor_timing_log_filename") == "reactor.log"
     assert p.get_double("nonlinear_convergence_coeff") == 0.1
+    f2 = tmp_path / "reactor.yml"
+    f2.write_text("constant_volume: 0\nalways_solve_temperature: 0\n"
+                  "solve_temperature_threshold: 5.0\n")
+    p.read_options_file(f2)
+    assert p.get_int("constant_volume") == 0 and p.get_int("always_solve_temperature") == 0
+    assert p.get_double("solve_temperature_threshold") == 5.0
     bad = tmp_path / "bad.yml"
     bad.write_text("max_steps: lots\n")
     with pytest.raises(PluginError) as e:
