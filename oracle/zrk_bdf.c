@@ -25,6 +25,13 @@
 #define MIN_FACTOR 0.2
 #define MAX_FACTOR 10.0
 #define ETA_KEEP 1.5
+/* CVODE's default per-step failure limits (the plugin sets neither
+ * CVodeSetMaxErrTestFails nor CVodeSetMaxConvFails): the 7th error-test
+ * failure or the 10th convergence failure within one step fails the attempt */
+#define MAX_NEF 7
+#define MAX_NCF 10
+#define MXNEF1 3       /* error-test failures before the order/step cut below */
+#define ETA_MIN_EF 0.1 /* step factor of that cut */
 
 static const double KAPPA[MAXO + 1] = {0.0, -0.1850, -1.0 / 9.0, -0.0823, -0.0415, 0.0};
 
@@ -44,6 +51,8 @@ void zo_bdf_default_opts(zo_bdf_opts *o) {
   o->retry_rtol = 1.0;
   o->dT_ign = 0.0;
   o->constant_volume = 1;
+  o->stop_ign = 0;
+  o->abstol_dens = 0;
 }
 
 typedef struct {
@@ -71,7 +80,15 @@ typedef struct {
    * within the call, the temperature at the last accepted step */
   double T_target, t_off, T_prev;
   double *t_ign;
+  double v0; /* initial inverse density (abstol_dens) */
 } bdf_t;
+
+/* absolute tolerance of component i (abstol_dens: reactor_nvector_serial.cpp:
+ * 107-119, correction 1 / (rho * (1 / W_k) * 1e-3)) */
+static double atol_of(const bdf_t *b, double atol, int i) {
+  if (!b->o->abstol_dens || i >= b->n - 1) return atol;
+  return atol * (1.0 / ((1.0 / b->v0) * (1.0 / b->r->t->mw[i]) * 1.0e-3));
+}
 
 static double rms(const double *x, const double *s, int n) {
   double a = 0.0;
@@ -240,7 +257,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
   memcpy(b->y, y0, sizeof(double) * n);
   if (rhs(b, 0.0, b->y, b->f0)) return -1;
   /* initial step: Hairer-Norsett-Wanner estimate (first order) */
-  for (int i = 0; i < n; ++i) b->scale[i] = atol + fabs(b->y[i]) * rtol;
+  for (int i = 0; i < n; ++i) b->scale[i] = atol_of(b, atol, i) + fabs(b->y[i]) * rtol;
   double d0 = rms(b->y, b->scale, n), d1 = rms(b->f0, b->scale, n);
   double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
   if (h0 > t_end) h0 = t_end;
@@ -264,6 +281,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
     if (nsteps_att >= o->max_steps) { rc = -4; goto failed; }
     int accepted = 0;
     double safety = 0.9, err_norm = 0.0;
+    int nef = 0, ncf = 0; /* this step's error-test and convergence failures */
     while (!accepted) {
       if (h > o->max_dt) { change_D(b, q, o->max_dt / h); h = o->max_dt; }
       if (t + h > t_end) {
@@ -280,7 +298,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
         double ps = 0.0;
         for (int k = 1; k <= q; ++k) ps += b->gam[k] * b->D[k * n + i];
         b->psi[i] = ps / b->alp[q];
-        b->scale[i] = atol + rtol * fabs(s);
+        b->scale[i] = atol_of(b, atol, i) + rtol * fabs(s);
       }
       const double c = h / b->alp[q];
       if (fabs(c / b->c_lu - 1.0) > 0.3)
@@ -315,6 +333,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
           if (factor(b, c)) { rc = -3; goto failed; }
           continue;
         }
+        if (++ncf >= MAX_NCF) { rc = -8; goto failed; }
         change_D(b, q, 0.5);
         h *= 0.5;
         b->st.nrej++;
@@ -325,10 +344,26 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
       err_norm = rms(b->err, b->scale, n);
       if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
+        if (++nef >= MAX_NEF) { rc = -9; goto failed; }
+        b->st.nrej++;
+        if (nef > MXNEF1) {
+          /* repeated failures (CVODE's rule, user guide sec. 2.1): order one
+           * lower and a tenth of the step; at order 1 the first difference
+           * is reloaded from f at the last accepted state */
+          if (q > 1) {
+            --q;
+            change_D(b, q, ETA_MIN_EF);
+          } else {
+            if (rhs(b, t, b->D, b->tmp)) { rc = -6; goto failed; }
+            for (int i = 0; i < n; ++i) b->D[n + i] = b->tmp[i] * (h * ETA_MIN_EF);
+          }
+          h *= ETA_MIN_EF;
+          neq = 0;
+          continue;
+        }
         double fac = fmax(MIN_FACTOR, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D(b, q, fac);
         h *= fac;
-        b->st.nrej++;
         continue;
       }
       accepted = 1;
@@ -338,7 +373,9 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
     nsteps_att++;
     neq++;
     b->jac_current = 0;
-    /* update differences */
+    /* update differences (stop_after_ignition keeps the previous state) */
+    const int keep_prev = b->t_ign && b->T_target > 0.0 && o->stop_ign && *b->t_ign < 0.0;
+    if (keep_prev) memcpy(b->tmp, b->D, sizeof(double) * n);
     for (int i = 0; i < n; ++i) {
       b->D[(q + 2) * n + i] = b->d[i] - b->D[(q + 1) * n + i];
       b->D[(q + 1) * n + i] = b->d[i];
@@ -350,6 +387,11 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
       if (*b->t_ign < 0.0 && Tn >= b->T_target) {
         const double frac = (Tn > b->T_prev) ? (b->T_target - b->T_prev) / (Tn - b->T_prev) : 1.0;
         *b->t_ign = b->t_off + (t - h) + frac * h;
+        if (o->stop_ign) { /* solver_cvode.cpp:259-263: the call ends at the crossing */
+          for (int i = 0; i < n; ++i) y0[i] = b->tmp[i] + frac * (b->D[i] - b->tmp[i]);
+          *t_done = (t - h) + frac * h;
+          return 0;
+        }
       }
       b->T_prev = Tn;
     }
@@ -422,6 +464,7 @@ int zo_reactor_solve(const zo_tables *t, const zo_jac_pattern *p, const zo_kinet
   b.r->cp = o->constant_volume == 0;
   b.r->fix_T = fix_T;
   zo_reactor_init_state(b.r, *T, *P, Y, dpdt, e_src, y_src);
+  b.v0 = b.r->inv_density;
   b.t_ign = t_ign;
   if (t_ign) *t_ign = -1.0;
   b.T_target = o->dT_ign > 0.0 ? *T + o->dT_ign : -1.0;

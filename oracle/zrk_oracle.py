@@ -59,7 +59,7 @@ class ZoBdfOpts(C.Structure):
                 ("min_mass_frac", C.c_double), ("step_limiter", C.c_double),
                 ("analytic", C.c_int), ("max_retries", C.c_int), ("retry_atol", C.c_double),
                 ("retry_rtol", C.c_double), ("dT_ign", C.c_double),
-                ("constant_volume", C.c_int)]
+                ("constant_volume", C.c_int), ("stop_ign", C.c_int), ("abstol_dens", C.c_int)]
 
 
 class ZoKinetics(C.Structure):

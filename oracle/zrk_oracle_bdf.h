@@ -43,6 +43,13 @@ typedef struct zo_bdf_opts {
   /* constant_volume: 1 constant-volume reactor, 0 constant-pressure reactor
    * (zerork_reactor_manager.cpp:85, :913-917) */
   int constant_volume;
+  /* stop_after_ignition (solver_cvode.cpp:259-263): with dT_ign > 0 the call
+   * ends at the first crossing, its state interpolated linearly between the
+   * two accepted steps around it */
+  int stop_ign;
+  /* abstol_dens (reactor_nvector_serial.cpp:107-119): the absolute tolerance
+   * of species k is abs_tol / (rho / W_k * 1e-3), rho the initial density */
+  int abstol_dens;
 } zo_bdf_opts;
 
 typedef struct zo_bdf_stats {

@@ -8,7 +8,7 @@ ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF_DATA = "/root/reference/data/mechanisms"
+from refpath import REF_DATA  # noqa: E402
 
 
 def pytest_configure(config):

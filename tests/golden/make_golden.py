@@ -27,7 +27,7 @@ sys.path.insert(0, ROOT)
 from zerork_b200 import mechgen  # noqa: E402
 import zrk_oracle as zo  # noqa: E402
 
-REF = "/root/reference/data/mechanisms"
+from refpath import REF_DATA as REF  # noqa: E402
 N_STATES = 12
 
 

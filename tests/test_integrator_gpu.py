@@ -153,7 +153,89 @@ def test_ignition_time(gpu, mech_dir):
     eo = np.abs(to - tt)[hit]
     eg = np.abs(ign - tt)[hit]
     assert np.all(eg <= 50 * np.maximum(eo, 10 * np.median(eo)) + 1e-3 * tt[hit]), (eg, eo)
-    assert np.all(ign[~hit] == -1.0)
+    # reactors that did not reach T0 + 400 K keep the caller's value (the
+    # reference sets the root time only when CVODE found one,
+    # zerork_reactor_manager.cpp:1128-1131)
+    assert np.all(ign[~hit] == -7.0)
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_stop_after_ignition(gpu, method, mech_dir):
+    """stop_after_ignition (solver_cvode.cpp:259-263): each reactor's call
+    ends at its ignition time, with the state interpolated linearly between
+    the accepted steps around the crossing, so T ends at T0 + 400 K; against
+    the oracle with the same option."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 16, "c1", seed=11)
+    p = Plugin(mf, tf, delta_temperature_ignition=400.0, stop_after_ignition=1, gpu_method=method)
+    ign = p.set_aux_field("IGNITION_TIME", np.full(16, -1.0))
+    Tg, Pg, Yg = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert p.solve(1e-3, Tg, Pg, Yg) == 0
+    hit = ign > 0
+    assert np.any(hit) and np.any(~hit)
+    np.testing.assert_allclose(Tg[hit], T[hit] + 400.0, rtol=0, atol=1e-6)
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    To, Po, Yo, so = ot.solve(T, P, Y, 1e-3, nthreads=os.cpu_count() or 1, dT_ign=400.0, stop_ign=1)
+    assert np.array_equal(so["t_ign"] > 0, hit)
+    np.testing.assert_allclose(To[hit], T[hit] + 400.0, rtol=0, atol=1e-6)
+    # ignition times and stopped states agree at the integration tolerance
+    assert np.all(np.abs(ign[hit] - so["t_ign"][hit]) <= 1e-4 * so["t_ign"][hit])
+    assert np.max(np.abs(Yg[hit] - Yo[hit])) < 1e-4
+    # the others ran the whole interval as without the option
+    q = Plugin(mf, tf, delta_temperature_ignition=400.0, gpu_method=method)
+    T2, P2, Y2 = T.copy(), P.copy(), np.ascontiguousarray(Y.copy())
+    assert q.solve(1e-3, T2, P2, Y2) == 0
+    assert np.array_equal(T2[~hit], Tg[~hit]) and np.array_equal(Y2[~hit], Yg[~hit])
+
+
+@pytest.mark.parametrize("method", [1, 2])
+def test_abstol_dens(gpu, method, mech_dir):
+    """abstol_dens = 1: species absolute tolerances abs_tol / (rho / W_k *
+    1e-3) (reactor_nvector_serial.cpp:107-119), with abs_tol 1e-12 (a
+    molar-concentration tolerance in mol/cm^3); against the oracle with the
+    same option and its tight-tolerance run, and different from the run
+    without the option."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 12, "c1", seed=11)
+    rc, Tg, Pg, Yg, p = _solve(mf, tf, T, P, Y, 1e-3, abstol_dens=1, abs_tol=1e-12, gpu_method=method)
+    assert rc == 0
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    nt = os.cpu_count() or 1
+    To, Po, Yo, so = ot.solve(T, P, Y, 1e-3, nthreads=nt, abstol_dens=1, atol=1e-12)
+    Tt, Pt, Yt, st = ot.solve(T, P, Y, 1e-3, nthreads=nt, rtol=1e-12, atol=1e-24, max_steps=400000)
+    ok = (so["status"] == 0) & (st["status"] == 0)
+    eo_T, eg_T = np.abs(To - Tt)[ok], np.abs(Tg - Tt)[ok]
+    assert np.all(eg_T <= 50 * np.maximum(eo_T, 10 * np.median(eo_T)) + 1e-5 * Tt[ok])
+    # the option changes the step sequence: steps differ from the default run
+    rc2, T2, P2, Y2, p2 = _solve(mf, tf, T, P, Y, 1e-3, abs_tol=1e-12, gpu_method=method)
+    assert p.last_stats()["nsteps"] != p2.last_stats()["nsteps"]
+
+
+def test_failure_caps_end_hopeless_attempts(gpu, mech_dir):
+    """CVODE's per-step limits (7 error-test, 10 convergence failures):
+    a reactor whose every attempt fails stops after a bounded number of
+    rejected steps instead of halving h until t + h == t.  A Newton
+    coefficient of 1e-12 makes every convergence test fail; the rejections
+    per attempt are then at most the cap."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    T, P, Y = mechgen.reactor_states(g, 4, "c1", seed=3)
+    p = Plugin(mf, tf, nonlinear_convergence_coeff=1e-30, cvode_num_retries=2)
+    Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+    rc = p.solve(1e-3, Tg, Pg, Yg, raise_on_fail=False)
+    assert rc == 7
+    st = p.last_stats()
+    assert st["nfailed"] == 4
+    # two attempts per reactor, each ending at the 10th convergence failure
+    # of its first step
+    assert st["nrej"] <= 4 * 2 * 10, st
 
 
 def _src_case(g, pm, n, seed):

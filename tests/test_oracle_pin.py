@@ -33,6 +33,7 @@ def _conc(tables, T, P, Y):
     ("ideal/sri_reaction.mech", "ideal/const_specific_heat.therm"),
     ("ideal/hydrogen_no_falloff.mech", "ideal/const_specific_heat.therm"),
     ("dme/dme_24_mech.txt", "dme/dme_24_therm.txt"),
+    ("n-heptane_reduced/heptanesymp159_mec.txt", "n-heptane_reduced/heptanesymp_therm.txt"),
 ])
 def test_oracle_matches_reference_library(mech, therm):
     m, t = os.path.join(REF_DATA, mech), os.path.join(REF_DATA, therm)

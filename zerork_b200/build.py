@@ -1,12 +1,14 @@
 """Build the sm_100a shared library in-tree: zerork_b200/lib/libzerork_b200.so.
 
 nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine
-with the CUDA 12.9 toolkit.  Object files are rebuilt when their source or any
-header in csrc/ is newer.
+with the CUDA 12.9 toolkit.  An object file is rebuilt when its source or a
+header it includes (directly or not) is newer; objects of sources that no
+longer exist are not linked.
 """
 import concurrent.futures as cf
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -34,11 +36,28 @@ def _flags(src):
     return ARCH + common
 
 
+_INC = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src, seen=None):
+    """The quoted includes of src, recursively (csrc/ and include/)."""
+    seen = set() if seen is None else seen
+    with open(src) as f:
+        text = f.read()
+    for name in _INC.findall(text):
+        for d in (os.path.dirname(src), CSRC, os.path.join(HERE, "..", "include")):
+            path = os.path.normpath(os.path.join(d, name))
+            if os.path.exists(path):
+                if path not in seen:
+                    seen.add(path)
+                    _deps(path, seen)
+                break
+    return seen
+
+
 def _compile(src, verbose=False):
     obj = os.path.join(OBJ, os.path.basename(src) + ".o")
-    headers = (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
-               glob.glob(os.path.join(HERE, "..", "include", "*.h")))
-    newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in headers])
+    newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _deps(src)])
     if os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj, None
     cmd = [nvcc(), "-c", src, "-o", obj] + _flags(src)

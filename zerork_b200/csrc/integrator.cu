@@ -478,7 +478,11 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
   // f0 = f(y0); initial step (Hairer-Norsett-Wanner)
   st.nrhs++;
   if (rhs_warp(m, o, w, v, t_off, V.y, V.f0, lane, false, nullptr)) return -1;
-  for (int i = lane; i < n; i += 32) V.scale[i] = atol + fabs(V.y[i]) * rtol;
+  // absolute tolerance of component i (abstol_dens: reactor_nvector_serial.cpp:107-119)
+  auto atol_of = [&](int i) {
+    return (o.abstol_dens && i < m.nsp) ? atol * (1.0 / ((1.0 / v) * m.inv_mw[i] * 1.0e-3)) : atol;
+  };
+  for (int i = lane; i < n; i += 32) V.scale[i] = atol_of(i) + fabs(V.y[i]) * rtol;
   __syncwarp();
   const double d0 = wrms_scaled(V.y, V.scale, n, lane), d1 = wrms_scaled(V.f0, V.scale, n, lane);
   double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
@@ -514,6 +518,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
     if (nsteps >= o.max_steps) { rc = -4; goto failed; }
     bool accepted = false;
     double safety = 0.9, err_norm = 0.0;
+    int nef = 0, ncf = 0;  // this step's error-test and convergence failures
     while (!accepted) {
       if (h > o.max_dt) {
         change_D(V.D, n, q, o.max_dt / h, lane);
@@ -531,7 +536,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
         for (int k = 1; k <= q; ++k) ps += bc.gam[k] * V.D[k * n + i];
         V.ypred[i] = s;
         V.psi[i] = ps / bc.alp[q];
-        V.scale[i] = atol + rtol * fabs(s);
+        V.scale[i] = atol_of(i) + rtol * fabs(s);
         V.y[i] = s;
         V.d[i] = 0.0;
       }
@@ -608,6 +613,7 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
           rank1_setup(c);
           continue;
         }
+        if (++ncf >= kMaxConvFails) { rc = -8; goto failed; }
         change_D(V.D, n, q, 0.5, lane);
         h *= 0.5;
         st.nrej++;
@@ -622,10 +628,25 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       err_norm = sqrt(wsum(a) / n);
       if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
+        if (++nef >= kMaxErrTestFails) { rc = -9; goto failed; }
+        st.nrej++;
+        if (nef > kErrFailsBeforeCut) {  // order and step cut (integrator.h)
+          if (q > 1) {
+            --q;
+            change_D(V.D, n, q, kEtaMinErrFail, lane);
+          } else {
+            st.nrhs++;
+            if (rhs_warp(m, o, w, v, t_off + t, V.D, V.tmp, lane, false, nullptr)) { rc = -6; goto failed; }
+            for (int i = lane; i < n; i += 32) V.D[n + i] = V.tmp[i] * (h * kEtaMinErrFail);
+            __syncwarp();
+          }
+          h *= kEtaMinErrFail;
+          neq = 0;
+          continue;
+        }
         const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D(V.D, n, q, fac, lane);
         h *= fac;
-        st.nrej++;
         continue;
       }
       accepted = true;
@@ -635,7 +656,9 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
     st.nsteps++;
     ++neq;
     jac_current = 0;
+    const bool keep_prev = T_target > 0.0 && o.stop_ign && t_ign < 0.0;
     for (int i = lane; i < n; i += 32) {
+      if (keep_prev) V.tmp[i] = V.D[i];  // the previous accepted state
       const double di = V.d[i];
       V.D[(q + 2) * n + i] = di - V.D[(q + 1) * n + i];
       V.D[(q + 1) * n + i] = di;
@@ -647,6 +670,12 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       if (t_ign < 0.0 && Tn >= T_target) {
         const double frac = (Tn > T_prev) ? (T_target - T_prev) / (Tn - T_prev) : 1.0;
         t_ign = t_off + (t - h) + frac * h;
+        if (o.stop_ign) {  // stop_after_ignition: the call ends at the crossing
+          for (int i = lane; i < n; i += 32) V.y[i] = V.tmp[i] + frac * (V.D[i] - V.tmp[i]);
+          __syncwarp();
+          t_done = (t - h) + frac * h;
+          return 0;
+        }
       }
       T_prev = Tn;
     }

@@ -21,6 +21,18 @@
 namespace zrk {
 
 constexpr int kMaxOrder = 5;
+// Per-step failure limits, CVODE's defaults (the plugin sets neither
+// CVodeSetMaxErrTestFails nor CVodeSetMaxConvFails, solver_cvode.cpp:51-212):
+// the 7th error-test failure or the 10th convergence failure (after a fresh
+// Jacobian) within one step fails the attempt, which then goes to the
+// plugin's retry loop.
+constexpr int kMaxErrTestFails = 7;
+constexpr int kMaxConvFails = 10;
+// From the 4th error-test failure within a step on, CVODE's rule (user
+// guide, sec. 2.1): the order drops by one and the step to a tenth; at
+// order 1 the first difference is reloaded from f at the last accepted state.
+constexpr int kErrFailsBeforeCut = 3;
+constexpr double kEtaMinErrFail = 0.1;
 
 struct LUDev {
   int n, nnz;
@@ -51,6 +63,11 @@ struct IntegOpts {
   double eps_lin;  // Krylov tolerance: eps_lin * nlscoef / error constant (WRMS)
   PredDev pred;    // learned predictor (dense integrator only; enabled = 0: off)
   double dT_ign;   // delta_temperature_ignition: > 0 records when T reaches T0 + dT_ign
+  int stop_ign;    // stop_after_ignition: the call ends at the crossing
+                   // (solver_cvode.cpp:259-263); its state is interpolated
+                   // linearly between the two accepted steps around it
+  int abstol_dens; // absolute tolerance of species k scaled by 1 / molar density
+                   // (reactor_nvector_serial.cpp:107-119)
 };
 
 // Per-reactor statistics written by the kernel.

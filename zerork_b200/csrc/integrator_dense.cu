@@ -1,5 +1,5 @@
 // integrator_dense.cu -- host side of the dense-block integrator: shared
-// memory layout and the launch dispatch over the register-chunk count.
+// memory layout and the launch dispatch over the factor type.
 #include "integrator_dense.cuh"
 
 namespace zrk {
@@ -29,19 +29,8 @@ cudaError_t launch_integrate_dense(const DevMech &m, const IntegOpts &o, const I
   const size_t smem = dense_smem_bytes(m, o.lu_fp32 != 0, &lda, spill);
   const int n = m.nsp + 1;
   if (n > kDenseMaxN) return cudaErrorInvalidValue;
-  // register chunks of 32 columns per lane in the inversion: ceil(n / 32)
-  const int nc = (n + 31) / 32;
-  switch (nc) {
-    case 1: return launch_integrate_dense_nc1(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 2: return launch_integrate_dense_nc2(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 3: return launch_integrate_dense_nc3(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 4: return launch_integrate_dense_nc4(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 5: return launch_integrate_dense_nc5(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 6: return launch_integrate_dense_nc6(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 7: return launch_integrate_dense_nc7(m, o, a, threads, ctas, spill, smem, lda, stream);
-    case 8: return launch_integrate_dense_nc8(m, o, a, threads, ctas, spill, smem, lda, stream);
-    default: return cudaErrorInvalidValue;
-  }
+  return o.lu_fp32 ? launch_integrate_dense_f32(m, o, a, threads, ctas, spill, smem, lda, stream)
+                   : launch_integrate_dense_f64(m, o, a, threads, ctas, spill, smem, lda, stream);
 }
 
 }  // namespace zrk

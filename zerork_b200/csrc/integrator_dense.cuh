@@ -98,7 +98,7 @@ __device__ __forceinline__ void source_cta(const DevMech &m, const IntegOpts &o,
 // Constant volume: reactor_constant_volume_cpu.cpp:64-128; constant pressure
 // (o.cp): reactor_constant_pressure_cpu.cpp:71-135, U then holds h/RT.
 // T_force > 0 replaces the energy-source temperature.
-__device__ __forceinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
+__device__ __noinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
                                        double v0, double t, const double *y, double *ydot,
                                        bool clamp, RhsOut *out, double T_force = 0.0) {
   const int S = m.nsp, tid = threadIdx.x, nt = blockDim.x;
@@ -167,7 +167,7 @@ __device__ __forceinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, con
 // right-hand side takes T from the energy, T* = T(E0 + esrc t, Y), which
 // this Jacobian does not see; the rank-one coupling g d^T (g = df/dT*,
 // d_j = dT*/dY_j = -e_j / c_x) goes to s.r1g / s.r1d for the Newton solves.
-__device__ __forceinline__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
+__device__ __noinline__ int jac_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
                                        double v0, double t, const double *y, const double *fy,
                                        double *J) {
   const int S = m.nsp, n = S + 1, tid = threadIdx.x, nt = blockDim.x;
@@ -285,7 +285,8 @@ __device__ __forceinline__ void warp_argmax(double &a, int &i, double &v, double
 }
 
 template <class LT, int NC>
-__device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda) {
+__device__ __noinline__ int invert_cta(const DevMech &m, const Smem &s, const double *J, double c, int n,
+                                       int lda) {
   LT *A = (LT *)s.A;
   LT *r1b = (LT *)s.colk;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, w = tid >> 5, nw = nt >> 5;
@@ -466,6 +467,22 @@ __device__ int invert_cta(const DevMech &m, const Smem &s, const double *J, doub
   return __syncthreads_or(bad);
 }
 
+// invert_cta for the register-chunk count nc = ceil(n / 32) (1..8).
+template <class LT>
+__device__ __forceinline__ int invert_any(int nc, const DevMech &m, const Smem &s, const double *J,
+                                          double c, int n, int lda) {
+  switch (nc) {
+    case 1: return invert_cta<LT, 1>(m, s, J, c, n, lda);
+    case 2: return invert_cta<LT, 2>(m, s, J, c, n, lda);
+    case 3: return invert_cta<LT, 3>(m, s, J, c, n, lda);
+    case 4: return invert_cta<LT, 4>(m, s, J, c, n, lda);
+    case 5: return invert_cta<LT, 5>(m, s, J, c, n, lda);
+    case 6: return invert_cta<LT, 6>(m, s, J, c, n, lda);
+    case 7: return invert_cta<LT, 7>(m, s, J, c, n, lda);
+    default: return invert_cta<LT, 8>(m, s, J, c, n, lda);
+  }
+}
+
 // x = (I - c_lu J)^{-1} b with the stored inverse: x = W A (perm of W^-1 b).
 // Thread per row, four independent partial sums to hide the FMA latency.
 template <class LT>
@@ -565,7 +582,7 @@ __device__ void make_consts(Consts &b) {
 template <class LT>
 // Under an energy source the operator and the preconditioner carry the
 // rank-one temperature coupling (r1k as in rank1_fix).
-__device__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda,
+__device__ __noinline__ int gmres_cta(const DevMech &m, const Smem &s, const double *J, double c, int n, int lda,
                          double delta, const double *b, double *x, int &iters, double r1k) {
   const int tid = threadIdx.x, nt = blockDim.x;
   const bool r1 = s.src.esrc != 0.0;
@@ -706,7 +723,7 @@ __device__ float *mlp_forward_cta(const MlpDev &net, float *a, float *b) {
 // without the network.  Inputs: log10 of the clamped mass fractions,
 // (T - 1500 K) / 1000 K, log10(P / 1 bar), log10(h); targets: change of
 // log10 mass fraction and (T' - T) / 100 K, standardised.
-__device__ void predict_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v, double h) {
+__device__ __noinline__ void predict_cta(const DevMech &m, const IntegOpts &o, const Smem &s, double v, double h) {
   const int S = m.nsp, n = S + 1, tid = threadIdx.x, nt = blockDim.x;
   const PredDev &p = o.pred;
   const double *y0 = s.D;
@@ -735,12 +752,13 @@ __device__ void predict_cta(const DevMech &m, const IntegOpts &o, const Smem &s,
   __syncthreads();
 }
 
-template <class LT, int NC>
+template <class LT>
 __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
                            double *J, double v, double t_end, double rtol, double atol,
                            ReactorStats &st, int lda, double &t_done, double t_off, double T_target,
                            double &t_ign) {
   const int n = m.nsp + 1, tid = threadIdx.x, nt = blockDim.x;
+  const int nc = (n + 31) / 32;
   auto vrms = [&](const double *x, const double *sc) {
     double a = 0.0;
     for (int i = tid; i < n; i += nt) {
@@ -754,6 +772,12 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
   t_done = 0.0;
   double T_prev = s.y[m.nsp] * o.Tref;  // ignition: temperature at the last accepted step
   double r1k = 0.0;  // energy-source coupling of the current factor
+  // absolute tolerance of component i: with abstol_dens the species' are
+  // abs_tol / molar density (reactor_nvector_serial.cpp:107-119, the
+  // correction formed as 1 / (rho / W_k * 1e-3)), at the initial density
+  auto atol_of = [&](int i) {
+    return (o.abstol_dens && i < m.nsp) ? atol * (1.0 / ((1.0 / v) * m.inv_mw[i] * 1.0e-3)) : atol;
+  };
   auto rank1_setup = [&](double cc) {
     if (s.src.esrc == 0.0) return;
     apply_inverse<LT>(s, n, lda, s.r1g, s.r1w);
@@ -764,7 +788,7 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
   };
   st.nrhs++;
   if (rhs_cta(m, o, s, v, t_off, s.y, s.f0, false, nullptr)) return -1;
-  for (int i = tid; i < n; i += nt) s.scale[i] = atol + fabs(s.y[i]) * rtol;
+  for (int i = tid; i < n; i += nt) s.scale[i] = atol_of(i) + fabs(s.y[i]) * rtol;
   __syncthreads();
   const double d0 = vrms(s.y, s.scale), d1 = vrms(s.f0, s.scale);
   double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
@@ -794,7 +818,7 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
   st.njac++;
   if (jac_cta(m, o, s, v, t_off, s.y, s.f0, J)) { rc = -2; goto failed; }
   st.nlu++;
-  if (invert_cta<LT, NC>(m, s, J, c_lu, n, lda)) { rc = -3; goto failed; }
+  if (invert_any<LT>(nc, m, s, J, c_lu, n, lda)) { rc = -3; goto failed; }
   rank1_setup(c_lu);
   while (t < t_end) {
     if (nsteps >= o.max_steps) { rc = -4; goto failed; }
@@ -805,6 +829,7 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
     // network for the rest of the attempt
     bool use_pred = o.pred.enabled != 0 && pred_fail < 2;
     double safety = 0.9, err_norm = 0.0;
+    int nef = 0, ncf = 0;  // this step's error-test and convergence failures
     while (!accepted) {
       if (h > o.max_dt) {
         change_D_cta(s.D, n, q, o.max_dt / h);
@@ -822,7 +847,7 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
         for (int k = 1; k <= q; ++k) ps += bc.gam[k] * s.D[k * n + i];
         s.ypred[i] = a;
         s.psi[i] = ps / bc.alp[q];
-        s.scale[i] = atol + rtol * fabs(a);
+        s.scale[i] = atol_of(i) + rtol * fabs(a);
         s.y[i] = a;
         s.d[i] = 0.0;
       }
@@ -836,7 +861,7 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
         st.nlu++;
         c_lu = c;
         crate = 1.0;
-        if (invert_cta<LT, NC>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
+        if (invert_any<LT>(nc, m, s, J, c, n, lda)) { rc = -3; goto failed; }
         rank1_setup(c);
       }
       const double gscale = (c == c_lu) ? 1.0 : 2.0 / (1.0 + c / c_lu);
@@ -905,10 +930,11 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
           st.nlu++;
           c_lu = c;
           crate = 1.0;
-          if (invert_cta<LT, NC>(m, s, J, c, n, lda)) { rc = -3; goto failed; }
+          if (invert_any<LT>(nc, m, s, J, c, n, lda)) { rc = -3; goto failed; }
           rank1_setup(c);
           continue;
         }
+        if (++ncf >= kMaxConvFails) { rc = -8; goto failed; }
         change_D_cta(s.D, n, q, 0.5);
         h *= 0.5;
         st.nrej++;
@@ -923,11 +949,26 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
       err_norm = sqrt(block_sum(a, s.red) / n);
       if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
+        if (++nef >= kMaxErrTestFails) { rc = -9; goto failed; }
         use_pred = false;
+        st.nrej++;
+        if (nef > kErrFailsBeforeCut) {  // order and step cut (integrator.h)
+          if (q > 1) {
+            --q;
+            change_D_cta(s.D, n, q, kEtaMinErrFail);
+          } else {
+            st.nrhs++;
+            if (rhs_cta(m, o, s, v, t_off + t, s.D, s.tmp, false, nullptr)) { rc = -6; goto failed; }
+            for (int i = tid; i < n; i += nt) s.D[n + i] = s.tmp[i] * (h * kEtaMinErrFail);
+            __syncthreads();
+          }
+          h *= kEtaMinErrFail;
+          neq = 0;
+          continue;
+        }
         const double fac = fmax(kMinFactor, safety * pow(err_norm, -1.0 / (q + 1)));
         change_D_cta(s.D, n, q, fac);
         h *= fac;
-        st.nrej++;
         continue;
       }
       if (use_pred) pred_fail = 0;  // the learned start converged and passed
@@ -938,7 +979,9 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
     st.nsteps++;
     ++neq;
     jac_current = 0;
+    const bool keep_prev = T_target > 0.0 && o.stop_ign && t_ign < 0.0;
     for (int i = tid; i < n; i += nt) {
+      if (keep_prev) s.tmp[i] = s.D[i];  // the previous accepted state
       const double di = s.d[i];
       s.D[(q + 2) * n + i] = di - s.D[(q + 1) * n + i];
       s.D[(q + 1) * n + i] = di;
@@ -950,6 +993,12 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
       if (t_ign < 0.0 && Tn >= T_target) {
         const double frac = (Tn > T_prev) ? (T_target - T_prev) / (Tn - T_prev) : 1.0;
         t_ign = t_off + (t - h) + frac * h;
+        if (o.stop_ign) {  // stop_after_ignition: the call ends at the crossing
+          for (int i = tid; i < n; i += nt) s.y[i] = s.tmp[i] + frac * (s.D[i] - s.tmp[i]);
+          __syncthreads();
+          t_done = (t - h) + frac * h;
+          return 0;
+        }
       }
       T_prev = Tn;
     }
@@ -998,7 +1047,7 @@ failed:  // D[0] holds the last accepted state (step-size changes keep it)
 
 // spill bits: 1 = rates of progress in a global slice, 2 = BDF differences
 // in a global slice (both L2-resident: one slice per resident CTA).
-template <class LT, int NC>
+template <class LT>
 __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, IntegOpts o, IntegArgs a,
                                                                  int lda, int spill) {
   extern __shared__ double smem_dyn[];
@@ -1082,7 +1131,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     s.ysrc = a.ysrc ? a.ysrc + (size_t)r * S : nullptr;
     for (int attempt = 0;; ++attempt) {
       double t_done = 0.0;
-      rc = attempt_cta<LT, NC>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done, a.dt - t_left,
+      rc = attempt_cta<LT>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done, a.dt - t_left,
                                T_target, t_ign);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
       t_left -= t_done;
@@ -1116,43 +1165,25 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
 }
 
 
-template <class LT, int NC>
+template <class LT>
 cudaError_t launch_dense(const DevMech &m, const IntegOpts &o, const IntegArgs &a, int threads,
                          int ctas, int spill, size_t smem, int lda, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(integrate_dense_kernel<LT, NC>,
+  cudaError_t e = cudaFuncSetAttribute(integrate_dense_kernel<LT>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  integrate_dense_kernel<LT, NC><<<ctas, threads, smem, stream>>>(m, o, a, lda, spill);
+  integrate_dense_kernel<LT><<<ctas, threads, smem, stream>>>(m, o, a, lda, spill);
   return cudaGetLastError();
 }
 
 }  // namespace
 
-// Launch for one register-chunk count NC = ceil((nsp + 1) / 32); one
-// translation unit per NC (integrator_dense_ncN.cu) so they compile in parallel.
-cudaError_t launch_integrate_dense_nc1(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc2(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc3(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc4(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc5(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc6(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc7(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
-cudaError_t launch_integrate_dense_nc8(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
-                                        int threads, int ctas, int spill, size_t smem, int lda,
-                                        cudaStream_t stream);
+// One translation unit per factor type (integrator_dense_f64.cu,
+// integrator_dense_f32.cu) so the two compile in parallel.
+cudaError_t launch_integrate_dense_f64(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                       int threads, int ctas, int spill, size_t smem, int lda,
+                                       cudaStream_t stream);
+cudaError_t launch_integrate_dense_f32(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                       int threads, int ctas, int spill, size_t smem, int lda,
+                                       cudaStream_t stream);
 
 }  // namespace zrk

@@ -1,0 +1,12 @@
+// integrator_dense_f64.cu -- dense-block integrator kernel with a double Newton factor.
+#include "integrator_dense.cuh"
+
+namespace zrk {
+
+cudaError_t launch_integrate_dense_f64(const DevMech &m, const IntegOpts &o, const IntegArgs &a,
+                                       int threads, int ctas, int spill, size_t smem, int lda,
+                                       cudaStream_t stream) {
+  return launch_dense<double>(m, o, a, threads, ctas, spill, smem, lda, stream);
+}
+
+}  // namespace zrk

@@ -213,6 +213,11 @@ static zrk::SolveOptions options_of(zerork_handle_impl *h) {
   o.dT_ign = D["delta_temperature_ignition"];
   o.constant_pressure = I["constant_volume"] == 0;  // zerork_reactor_manager.cpp:913-917
   o.always_solve_T = I["always_solve_temperature"] != 0;  // :1107-1113
+  // solver_cvode.cpp:262 and reactor_nvector_serial.cpp:107-119; the
+  // reference's defaults table has no stop_after_ignition entry (unset = 0)
+  auto si = I.find("stop_after_ignition");
+  o.stop_after_ignition = si != I.end() && si->second != 0;
+  o.abstol_dens = I["abstol_dens"] != 0;
   return o;
 }
 

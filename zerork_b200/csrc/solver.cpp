@@ -215,6 +215,8 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   io.lu_fp32 = o.lu_fp32 ? 1 : 0;
   io.cp = o.constant_pressure ? 1 : 0;
   io.always_T = o.always_solve_T ? 1 : 0;
+  io.stop_ign = (o.stop_after_ignition && o.dT_ign > 0.0) ? 1 : 0;
+  io.abstol_dens = o.abstol_dens ? 1 : 0;
   IntegArgs a;
   std::memset(&a, 0, sizeof(a));
   a.n_reactors = n;
@@ -232,7 +234,9 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   a.stats = dstats_;
   a.rop_scratch = drop_;
   a.ysrc = ysrc ? dsrc_ : nullptr;
-  a.t_ign = (t_ign && o.dT_ign > 0.0) ? dign_ : nullptr;
+  // ignition times are tracked whenever delta_temperature_ignition > 0 (the
+  // stop_after_ignition option needs them even without a caller field)
+  a.t_ign = (o.dT_ign > 0.0) ? dign_ : nullptr;
   a.dpdt = dpdt ? dde_ : nullptr;
   a.esrc = esrc ? dde_ + cap_ : nullptr;
   a.tdel_in = (!o.always_solve_T && temp_delta) ? dde_ + 2 * cap_ : nullptr;
@@ -310,7 +314,6 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
   ++graph_launches;
   std::memcpy(T, hT_, n * sizeof(double));
   std::memcpy(P, hP_, n * sizeof(double));
-  if (a.t_ign) std::memcpy(t_ign, hign_, n * sizeof(double));
   const ReactorStats *st = hstats_;
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) {
@@ -322,6 +325,10 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     const ReactorStats &q = st[r];
     if (q.status == 0) {
       std::memcpy(mf + (size_t)r * stride, &Y[(size_t)r * S], S * sizeof(double));
+      // the root time of a reactor that integrated and crossed T0 + dT in
+      // this call (zerork_reactor_manager.cpp:1128-1131 sets it only for
+      // reactors that integrated); otherwise the caller's value stays
+      if (t_ign && a.t_ign && hign_[r] >= 0.0) t_ign[r] = hign_[r];
       if (temp_delta) {
         double d = T[r] - T0[r];
         temp_delta[r] = (d < temp_threshold) ? 0.0 : d;

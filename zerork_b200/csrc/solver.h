@@ -38,6 +38,8 @@ struct SolveOptions {
   bool constant_pressure = false;  // plugin option constant_volume = 0
   bool always_solve_T = true;      // always_solve_temperature; false: reactors whose
                                    // input temperature delta is <= 0 keep T fixed
+  bool stop_after_ignition = false;  // end each reactor's call at its ignition time
+  bool abstol_dens = false;          // species absolute tolerances / molar density
 };
 
 struct SolveStatsTotals {
@@ -58,7 +60,9 @@ class ReactorSolver {
   // cost/gpu_time/temp_delta may be null.  Returns the number of failed
   // reactors (state left unchanged for those), or -1 on a CUDA error.
   // ysrc: optional mass-fraction sources [n][nsp] (1/s); t_ign: optional
-  // ignition times [n] (written when o.dT_ign > 0, -1 where not reached);
+  // ignition times [n] (when o.dT_ign > 0, written for the reactors that
+  // integrated and reached T0 + dT_ign in this call; left as they were
+  // otherwise);
   // dpdt, esrc: optional pressure rates (Pa/s) and energy sources (J/kg/s) [n].
   int solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
             int stride, double *cost, double *gpu_time, double *temp_delta,
