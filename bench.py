@@ -255,11 +255,7 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
 def _oracle_tables(pm, zo):
     """CPU oracle tables from the product loader's tables (the loader is pinned
     bit-exact to the reference's own tables by the test suite)."""
-    d = pm.tables()
-    d.update(tot_reac=len(d["reac_spc"]), tot_prod=len(d["prod_spc"]), n_arr=len(d["arr_step"]),
-             n_keq=len(d["keq_step"]), n_tb=len(d["tb_fwd"]), n_fo=len(d["fo_fwd"]),
-             n_tb_eff=len(d["tb_spc"]), n_fo_eff=len(d["fo_eff_spc"]))
-    return zo.OracleTables(d)
+    return zo.OracleTables(zo.with_counts(pm.tables()))
 
 
 def run_reference_arm(a, rank, world):

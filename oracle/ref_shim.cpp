@@ -53,7 +53,7 @@ zo_tables *zrkref_tables(void *hp) {
   zerork::info_net *inf = m->infoNet;
   zerork::rate_const *rc = m->Kconst;
   const int nsp = m->getNumSpecies(), nstep = m->getNumSteps();
-  int s[11];
+  int s[14];
   s[0] = nsp;
   s[1] = m->getNumReactions();
   s[2] = nstep;
@@ -69,6 +69,15 @@ zo_tables *zrkref_tables(void *hp) {
     if (rc->falloffRxnList[j].falloffSpcIdx < 0) nfoe += rc->falloffRxnList[j].nEnhanced;
   s[9] = ntbe;
   s[10] = nfoe;
+  // PLOG reactions: the reference's PLogReaction objects (plog_reaction.h)
+  int npt = 0, nln = 0;
+  for (int j = 0; j < rc->nPLogInterpolationStep; ++j) {
+    npt += rc->plogInterpolationStepList[j].num_pressure_points_;
+    nln += rc->plogInterpolationStepList[j].total_arrhenius_lines_;
+  }
+  s[11] = rc->nPLogInterpolationStep;
+  s[12] = npt;
+  s[13] = nln;
   zo_tables *t = zo_tables_alloc(s);
   m->getMolWtSpc(t->mw);
   std::vector<double> coef(nsp * 16);
@@ -143,6 +152,26 @@ zo_tables *zrkref_tables(void *hp) {
     }
   }
   t->fo_ptr[rc->nFalloffRxn] = e;
+  int q = 0, l = 0;
+  for (int j = 0; j < rc->nPLogInterpolationStep; ++j) {
+    const zerork::PLogReaction &pr = rc->plogInterpolationStepList[j];
+    t->plog_step[j] = pr.step_index_;
+    t->plog_pt_ptr[j] = q;
+    for (int k = 0; k < pr.num_pressure_points_; ++k, ++q) {
+      t->plog_p[q] = pr.pressure_points_[k];
+      t->plog_lnp[q] = pr.log_e_pressure_points_[k];
+      t->plog_ln_ptr[q] = l + pr.start_line_at_pressure_[k];
+    }
+    for (int k = 0; k < pr.total_arrhenius_lines_; ++k) {
+      t->plog_lnA[l + k] = pr.log_e_afactor_[k];
+      t->plog_sgn[l + k] = pr.sign_afactor_[k];
+      t->plog_n[l + k] = pr.temperature_power_[k];
+      t->plog_Ta[l + k] = pr.activation_temperature_[k];
+    }
+    l += pr.total_arrhenius_lines_;
+  }
+  t->plog_pt_ptr[rc->nPLogInterpolationStep] = q;
+  t->plog_ln_ptr[npt] = l;
   return t;
 }
 

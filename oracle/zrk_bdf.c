@@ -53,6 +53,7 @@ void zo_bdf_default_opts(zo_bdf_opts *o) {
   o->constant_volume = 1;
   o->stop_ign = 0;
   o->abstol_dens = 0;
+  o->fail_caps = 1;
 }
 
 typedef struct {
@@ -333,7 +334,7 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
           if (factor(b, c)) { rc = -3; goto failed; }
           continue;
         }
-        if (++ncf >= MAX_NCF) { rc = -8; goto failed; }
+        if (++ncf >= MAX_NCF && o->fail_caps) { rc = -8; goto failed; }
         change_D(b, q, 0.5);
         h *= 0.5;
         b->st.nrej++;
@@ -344,9 +345,9 @@ static int integrate(bdf_t *b, double *y0, double t_end, double rtol, double ato
       err_norm = rms(b->err, b->scale, n);
       if (!isfinite(err_norm)) { rc = -7; goto failed; }
       if (err_norm > 1.0) {
-        if (++nef >= MAX_NEF) { rc = -9; goto failed; }
+        if (++nef >= MAX_NEF && o->fail_caps) { rc = -9; goto failed; }
         b->st.nrej++;
-        if (nef > MXNEF1) {
+        if (nef > MXNEF1 && o->fail_caps) {
           /* repeated failures (CVODE's rule, user guide sec. 2.1): order one
            * lower and a tenth of the step; at order 1 the first difference
            * is reloaded from f at the last accepted state */

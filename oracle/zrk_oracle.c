@@ -16,7 +16,7 @@
 
 static void *zcalloc(size_t n, size_t sz) { return calloc(n > 0 ? n : 1, sz); }
 
-zo_tables *zo_tables_alloc(const int s[11]) {
+zo_tables *zo_tables_alloc(const int s[14]) {
   zo_tables *t = (zo_tables *)zcalloc(1, sizeof(zo_tables));
   t->nsp = s[0]; t->nrxn = s[1]; t->nstep = s[2];
   t->tot_reac = s[3]; t->tot_prod = s[4];
@@ -50,6 +50,16 @@ zo_tables *zo_tables_alloc(const int s[11]) {
   t->fo_eff_spc = (int *)zcalloc(t->n_fo_eff, sizeof(int));
   t->fo_alpha = (double *)zcalloc(t->n_fo_eff, sizeof(double));
   t->fo_par = (double *)zcalloc((size_t)t->n_fo * 8, sizeof(double));
+  t->n_plog = s[11]; t->n_plog_pt = s[12]; t->n_plog_ln = s[13];
+  t->plog_step = (int *)zcalloc(t->n_plog, sizeof(int));
+  t->plog_pt_ptr = (int *)zcalloc(t->n_plog + 1, sizeof(int));
+  t->plog_ln_ptr = (int *)zcalloc(t->n_plog_pt + 1, sizeof(int));
+  t->plog_p = (double *)zcalloc(t->n_plog_pt, sizeof(double));
+  t->plog_lnp = (double *)zcalloc(t->n_plog_pt, sizeof(double));
+  t->plog_lnA = (double *)zcalloc(t->n_plog_ln, sizeof(double));
+  t->plog_sgn = (double *)zcalloc(t->n_plog_ln, sizeof(double));
+  t->plog_n = (double *)zcalloc(t->n_plog_ln, sizeof(double));
+  t->plog_Ta = (double *)zcalloc(t->n_plog_ln, sizeof(double));
   return t;
 }
 
@@ -62,6 +72,8 @@ void zo_tables_free(zo_tables *t) {
   free(t->tb_fwd); free(t->tb_rev); free(t->tb_ptr); free(t->tb_spc); free(t->tb_alpha);
   free(t->fo_fwd); free(t->fo_rev); free(t->fo_type); free(t->fo_spc); free(t->fo_ptr);
   free(t->fo_eff_spc); free(t->fo_alpha); free(t->fo_par);
+  free(t->plog_step); free(t->plog_pt_ptr); free(t->plog_ln_ptr); free(t->plog_p);
+  free(t->plog_lnp); free(t->plog_lnA); free(t->plog_sgn); free(t->plog_n); free(t->plog_Ta);
   free(t);
 }
 
@@ -115,6 +127,34 @@ void zo_g_RT(const zo_tables *t, double T, double *g_RT) {
 }
 
 /* ------------------------------------------------------- rate coefficients */
+/* A PLOG reaction at (T, P): plog_reaction.cpp:166-185 (the Arrhenius lines
+ * of one pressure, summed with the sign of A) and :187-300 (no
+ * extrapolation: the end pressures' values outside [p_min, p_max];
+ * logarithmic interpolation inside; zero for T or P <= 0 or a non-positive
+ * bracketing value). */
+static double plog_at(const zo_tables *t, int q, double invT, double logT) {
+  double k = 0.0;
+  for (int l = t->plog_ln_ptr[q]; l < t->plog_ln_ptr[q + 1]; ++l)
+    k += t->plog_sgn[l] * exp(t->plog_lnA[l] + logT * t->plog_n[l] - invT * t->plog_Ta[l]);
+  return k;
+}
+
+double zo_plog_k(const zo_tables *t, int j, double T, double invT, double logT, double P) {
+  const int q0 = t->plog_pt_ptr[j], q1 = t->plog_pt_ptr[j + 1];
+  if (T <= 0.0 || P <= 0.0) return 0.0;
+  if (q1 - q0 == 1) return plog_at(t, q0, invT, logT);
+  if (P <= t->plog_p[q0]) return plog_at(t, q0, invT, logT);
+  if (P >= t->plog_p[q1 - 1]) return plog_at(t, q1 - 1, invT, logT);
+  int r = q0;
+  while (r + 1 < q1 - 1 && !(t->plog_p[r] <= P && P < t->plog_p[r + 1])) ++r;
+  const double k1 = plog_at(t, r, invT, logT);
+  if (k1 <= 0.0) return 0.0;
+  const double k2 = plog_at(t, r + 1, invT, logT);
+  if (k2 <= 0.0) return 0.0;
+  const double e = log(k2 / k1) / (t->plog_lnp[r + 1] - t->plog_lnp[r]);
+  return k1 * pow(P / t->plog_p[r], e);
+}
+
 /* rate_const.cpp:539-582 updateK, with updateArrheniusStep (:669-687),
  * updateFromKeqStep (:690-731), updateThirdBodyRxn (:862-888) and
  * updateFalloffRxn (:890-1012).  Exponentials use libc exp (the
@@ -132,6 +172,10 @@ void zo_rate_coefs(const zo_tables *t, double T, const double *C, double *K) {
     double a = t->arr_lnA[j] + t->arr_n[j] * logT - t->arr_Ta[j] * invT;
     K[t->arr_step[j]] = exp(a);
   }
+  /* PLOG steps before the reverse rates (rate_const.cpp:565-567), at the
+   * pressure of the concentrations, Csum Ru T */
+  for (int j = 0; j < t->n_plog; ++j)
+    K[t->plog_step[j]] = zo_plog_k(t, j, T, invT, logT, Csum * ZO_RU * T);
   if (t->n_keq > 0) {
     double *g = (double *)malloc(sizeof(double) * nsp);
     zo_g_RT(t, T, g);
@@ -630,11 +674,14 @@ int zo_jac_values(zo_reactor *r, const zo_jac_pattern *p, const double *y, const
     jac[lr] *= RuTemp;
     if (scale) scale[lr] = sc * fabs(RuTemp);
   }
+  /* the Tdot term carries Tdot's own rounding: its scale is the magnitude
+   * sum of Tdot's terms (yscale of the clamped evaluation), not |Tdot|, which
+   * cancellation can make far smaller */
   for (int j = 0; j < ns; ++j) {
     int lr = p->last_row[j];
     double add = t3[ns] * r->cv_spc[j] * mw[j];
     jac[lr] += add;
-    if (scale) scale[lr] += fabs(add);
+    if (scale) scale[lr] += fabs(r->yscale[ns] * r->cv_spc[j] * mw[j]);
   }
   const double multFact = -1.0 / (r->mean_cv);
   for (int j = 0; j < ns; ++j) {

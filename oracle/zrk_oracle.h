@@ -40,6 +40,7 @@ typedef struct zo_tables {
   int nsp, nrxn, nstep;
   int tot_reac, tot_prod;
   int n_arr, n_keq, n_tb, n_fo, n_tb_eff, n_fo_eff;
+  int n_plog, n_plog_pt, n_plog_ln;
   double *mw;        /* [nsp] kg/kmol */
   double *thermo;    /* [nsp*16]: Tmid, 7 low, 7 high, pad */
   int *step_rxn;     /* [nstep] */
@@ -56,10 +57,21 @@ typedef struct zo_tables {
   double *tb_alpha;
   int *fo_fwd, *fo_rev, *fo_type, *fo_spc, *fo_ptr, *fo_eff_spc;  /* fo_spc=-1 => M */
   double *fo_alpha, *fo_par;
+  /* PLOG reactions (plog_reaction.cpp:8-132, rate_const.cpp:1146-1185): the
+   * forward step, distinct pressures [plog_pt_ptr[j], plog_pt_ptr[j+1]) in Pa
+   * (ascending) with their logs, and per pressure the Arrhenius lines
+   * [plog_ln_ptr[q], plog_ln_ptr[q+1]): ln|A|, sign of A, n, Ta */
+  int *plog_step, *plog_pt_ptr, *plog_ln_ptr;
+  double *plog_p, *plog_lnp, *plog_lnA, *plog_sgn, *plog_n, *plog_Ta;
 } zo_tables;
 
-zo_tables *zo_tables_alloc(const int sizes[11]); /* nsp,nrxn,nstep,tot_reac,tot_prod,
-                                                   n_arr,n_keq,n_tb,n_fo,n_tb_eff,n_fo_eff */
+zo_tables *zo_tables_alloc(const int sizes[14]); /* nsp,nrxn,nstep,tot_reac,tot_prod,
+                                                   n_arr,n_keq,n_tb,n_fo,n_tb_eff,n_fo_eff,
+                                                   n_plog,n_plog_pt,n_plog_ln */
+/* A PLOG reaction's rate coefficient at (T, P) (plog_reaction.cpp:187-300,
+ * logarithmic interpolation between the bracketing pressures, the end
+ * pressures' values outside them) */
+double zo_plog_k(const zo_tables *t, int j, double T, double invT, double logT, double P);
 void zo_tables_free(zo_tables *t);
 
 /* Physical constants: src/zerork/constants.h:10-24 */

@@ -25,7 +25,7 @@ _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 class ZoTables(C.Structure):
     _fields_ = [(n, C.c_int) for n in (
         "nsp", "nrxn", "nstep", "tot_reac", "tot_prod", "n_arr", "n_keq", "n_tb",
-        "n_fo", "n_tb_eff", "n_fo_eff")] + [
+        "n_fo", "n_tb_eff", "n_fo_eff", "n_plog", "n_plog_pt", "n_plog_ln")] + [
         ("mw", C.POINTER(C.c_double)), ("thermo", C.POINTER(C.c_double)),
         ("step_rxn", C.POINTER(C.c_int)), ("step_dir", C.POINTER(C.c_int)),
         ("reac_ptr", C.POINTER(C.c_int)), ("reac_spc", C.POINTER(C.c_int)),
@@ -41,6 +41,11 @@ class ZoTables(C.Structure):
         ("fo_type", C.POINTER(C.c_int)), ("fo_spc", C.POINTER(C.c_int)),
         ("fo_ptr", C.POINTER(C.c_int)), ("fo_eff_spc", C.POINTER(C.c_int)),
         ("fo_alpha", C.POINTER(C.c_double)), ("fo_par", C.POINTER(C.c_double)),
+        ("plog_step", C.POINTER(C.c_int)), ("plog_pt_ptr", C.POINTER(C.c_int)),
+        ("plog_ln_ptr", C.POINTER(C.c_int)), ("plog_p", C.POINTER(C.c_double)),
+        ("plog_lnp", C.POINTER(C.c_double)), ("plog_lnA", C.POINTER(C.c_double)),
+        ("plog_sgn", C.POINTER(C.c_double)), ("plog_n", C.POINTER(C.c_double)),
+        ("plog_Ta", C.POINTER(C.c_double)),
     ]
 
 
@@ -59,7 +64,8 @@ class ZoBdfOpts(C.Structure):
                 ("min_mass_frac", C.c_double), ("step_limiter", C.c_double),
                 ("analytic", C.c_int), ("max_retries", C.c_int), ("retry_atol", C.c_double),
                 ("retry_rtol", C.c_double), ("dT_ign", C.c_double),
-                ("constant_volume", C.c_int), ("stop_ign", C.c_int), ("abstol_dens", C.c_int)]
+                ("constant_volume", C.c_int), ("stop_ign", C.c_int), ("abstol_dens", C.c_int),
+                ("fail_caps", C.c_int)]
 
 
 class ZoKinetics(C.Structure):
@@ -89,9 +95,14 @@ TABLE_ARRAYS = {
     "fo_type": ("i4", lambda t: t.n_fo), "fo_spc": ("i4", lambda t: t.n_fo),
     "fo_ptr": ("i4", lambda t: t.n_fo + 1), "fo_eff_spc": ("i4", lambda t: t.n_fo_eff),
     "fo_alpha": ("f8", lambda t: t.n_fo_eff), "fo_par": ("f8", lambda t: 8 * t.n_fo),
+    "plog_step": ("i4", lambda t: t.n_plog), "plog_pt_ptr": ("i4", lambda t: t.n_plog + 1),
+    "plog_ln_ptr": ("i4", lambda t: t.n_plog_pt + 1), "plog_p": ("f8", lambda t: t.n_plog_pt),
+    "plog_lnp": ("f8", lambda t: t.n_plog_pt), "plog_lnA": ("f8", lambda t: t.n_plog_ln),
+    "plog_sgn": ("f8", lambda t: t.n_plog_ln), "plog_n": ("f8", lambda t: t.n_plog_ln),
+    "plog_Ta": ("f8", lambda t: t.n_plog_ln),
 }
 TABLE_COUNTS = ("nsp", "nrxn", "nstep", "tot_reac", "tot_prod", "n_arr", "n_keq", "n_tb",
-                "n_fo", "n_tb_eff", "n_fo_eff")
+                "n_fo", "n_tb_eff", "n_fo_eff", "n_plog", "n_plog_pt", "n_plog_ln")
 
 
 def _bind_common(lib):
@@ -201,6 +212,22 @@ def _reactor_rhs(fn, nsp, cp, T0, P0, Y0, tm, y, dpdt, e_src, y_src):
     return ydot
 
 
+def with_counts(d):
+    """A table dict (e.g. the product loader's tables) with the size fields
+    the oracle's struct needs, derived from the array lengths."""
+    d = dict(d)
+    d.update(tot_reac=len(d["reac_spc"]), tot_prod=len(d["prod_spc"]), n_arr=len(d["arr_step"]),
+             n_keq=len(d["keq_step"]), n_tb=len(d["tb_fwd"]), n_fo=len(d["fo_fwd"]),
+             n_tb_eff=len(d["tb_spc"]), n_fo_eff=len(d["fo_eff_spc"]),
+             n_plog=len(d.get("plog_step", ())), n_plog_pt=len(d.get("plog_p", ())),
+             n_plog_ln=len(d.get("plog_lnA", ())))
+    for k in ("plog_step", "plog_p", "plog_lnp", "plog_lnA", "plog_sgn", "plog_n", "plog_Ta"):
+        d.setdefault(k, np.zeros(0))
+    d.setdefault("plog_pt_ptr", np.zeros(1, dtype=np.int32))
+    d.setdefault("plog_ln_ptr", np.zeros(1, dtype=np.int32))
+    return d
+
+
 def tables_to_dict(tp):
     t = tp.contents
     d = {n: getattr(t, n) for n in TABLE_COUNTS}
@@ -216,7 +243,7 @@ class OracleTables:
 
     def __init__(self, d, lib=None):
         self.lib = lib or oracle_lib()
-        sizes = (C.c_int * 11)(*[int(d[n]) for n in TABLE_COUNTS])
+        sizes = (C.c_int * 14)(*[int(d[n]) for n in TABLE_COUNTS])
         self.ptr = self.lib.zo_tables_alloc(sizes)
         t = self.ptr.contents
         for name, (dt, size) in TABLE_ARRAYS.items():

@@ -50,6 +50,12 @@ typedef struct zo_bdf_opts {
   /* abstol_dens (reactor_nvector_serial.cpp:107-119): the absolute tolerance
    * of species k is abs_tol / (rho / W_k * 1e-3), rho the initial density */
   int abstol_dens;
+  /* 1: CVODE's per-step failure limits (7 error-test, 10 convergence
+   * failures fail the attempt) and its order/step cut after the 3rd
+   * error-test failure, as the plugin runs; 0: neither (tight-tolerance
+   * reference runs, where the energy inversion's 1e-6 K stop is a noise
+   * floor that makes repeated rejections normal) */
+  int fail_caps;
 } zo_bdf_opts;
 
 typedef struct zo_bdf_stats {

@@ -68,11 +68,7 @@ def oracle_tables(pm):
     """Oracle tables fed with the product loader's tables (pinned bit-exact to
     the reference's own by tests/test_loader.py)."""
     import zrk_oracle as zo
-    d = pm.tables()
-    d.update(tot_reac=len(d["reac_spc"]), tot_prod=len(d["prod_spc"]), n_arr=len(d["arr_step"]),
-             n_keq=len(d["keq_step"]), n_tb=len(d["tb_fwd"]), n_fo=len(d["fo_fwd"]),
-             n_tb_eff=len(d["tb_spc"]), n_fo_eff=len(d["fo_eff_spc"]))
-    return zo.OracleTables(d)
+    return zo.OracleTables(zo.with_counts(pm.tables()))
 
 
 def scaled_err(a, b, scale, floor=1e-300):

@@ -25,7 +25,9 @@ SHIPPED = [
     ("ideal/hydrogen_recombination_rev_zero.mech", "ideal/const_specific_heat.therm"),
     ("ideal/hydrogen_no_falloff.mech", "ideal/const_specific_heat.therm"),
     ("dme/dme_24_mech.txt", "dme/dme_24_therm.txt"),
-    ("n-heptane_reduced/heptanesymp159_mec.txt", "n-heptane_reduced/heptanesymp159_therm.txt"),
+    ("n-heptane_reduced/heptanesymp159_mec.txt", "n-heptane_reduced/heptanesymp_therm.txt"),
+    ("plog/plog_test.mech", "plog/plog_test.therm"),
+    ("ideal/plog_test.mech", "ideal/const_specific_heat.therm"),
 ]
 
 
@@ -78,11 +80,18 @@ def test_parse_errors(tmp_path, c1):
     with pytest.raises(zb.ZeroRKError) as e:
         zb.Mechanism(str(tmp_path / "missing.mech"), tf, device=False)
     assert e.value.code == 3
-    bad = tmp_path / "plog.mech"
+    bad = tmp_path / "ford.mech"
     bad.write_text("ELEMENTS\nH\nEND\nSPECIES\nH H2\nEND\nREACTIONS\n"
-                   "H2 <=> H + H 1e10 0 0\n PLOG / 1.0 1e10 0 0 /\nEND\n")
-    with pytest.raises(zb.ZeroRKError, match="PLOG"):
+                   "H2 <=> H + H 1e10 0 0\n FORD / H2 0.5 /\nEND\n")
+    with pytest.raises(zb.ZeroRKError, match="FORD"):
         zb.Mechanism(str(bad), tf, device=False)
+    # PLOG excludes third-body data and REV (CKParser.cpp:312-350)
+    for extra, msg in (("H2 + M <=> H + H + M 1e10 0 0\n PLOG / 1.0 1e10 0 0 /\n", "third-body"),
+                       ("H2 <=> H + H 1e10 0 0\n PLOG / 1.0 1e10 0 0 /\n REV / 1e10 0 0 /\n", "REV")):
+        bad = tmp_path / "plog_bad.mech"
+        bad.write_text("ELEMENTS\nH\nEND\nSPECIES\nH H2\nEND\nREACTIONS\n" + extra + "END\n")
+        with pytest.raises(zb.ZeroRKError, match=msg):
+            zb.Mechanism(str(bad), tf, device=False)
     und = tmp_path / "und.mech"
     und.write_text("ELEMENTS\nH\nEND\nSPECIES\nH2\nEND\nREACTIONS\nH2 <=> HX + HX 1e10 0 0\nEND\n")
     with pytest.raises(zb.ZeroRKError, match="undeclared"):

@@ -95,7 +95,7 @@ def test_oracle_bdf_sources_match_scipy_radau(cv, mech_dir):
     T, P, Y = T[1:], P[1:], Y[1:]
     dpdt, esrc, dt = np.array([2.6e6]), np.array([7.6e7]), 5e-4
     To, Po, Yo, so = ot.solve(T, P, Y, dt, dpdt=dpdt, e_src=esrc, constant_volume=cv,
-                              rtol=1e-10, atol=1e-22, max_steps=400000)
+                              rtol=1e-10, atol=1e-22, max_steps=400000, fail_caps=0)
     assert so["status"][0] == 0
 
     def f(t, y):
@@ -106,3 +106,24 @@ def test_oracle_bdf_sources_match_scipy_radau(cv, mech_dir):
     assert sol.status == 0
     assert abs(sol.y[-1, -1] - To[0]) < 5e-3, (sol.y[-1, -1], To[0])
     assert np.max(np.abs(sol.y[:-1, -1] - Yo[0])) < 1e-6
+
+
+def test_oracle_per_step_failure_limits(mech_dir):
+    """CVODE's per-step limits (7 error-test, 10 convergence failures per
+    step; order and step cut after the 3rd error-test failure) end an
+    attempt that the energy inversion's 1e-6 K noise floor keeps rejecting
+    at rtol 1e-10: with the limits the constant-pressure reactor with
+    pressure-rate and energy sources needs retries (or fails), without them
+    it grinds through in one attempt."""
+    import zerork_b200 as zb
+    from zerork_b200 import mechgen
+    g, (mf, tf) = synth("c1_h2", mech_dir)
+    ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
+    T, P, Y = mechgen.reactor_states(g, 2, "c1", seed=23)
+    T, P, Y = T[1:], P[1:], Y[1:]
+    src = dict(dpdt=np.array([2.6e6]), e_src=np.array([7.6e7]), constant_volume=0, rtol=1e-10,
+               atol=1e-22, max_steps=400000)
+    _, _, _, capped = ot.solve(T, P, Y, 5e-4, **src)
+    _, _, _, free = ot.solve(T, P, Y, 5e-4, fail_caps=0, **src)
+    assert free["status"][0] == 0 and free["retries"][0] == 0
+    assert capped["status"][0] != 0 or capped["retries"][0] > 0

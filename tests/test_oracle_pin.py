@@ -34,6 +34,8 @@ def _conc(tables, T, P, Y):
     ("ideal/hydrogen_no_falloff.mech", "ideal/const_specific_heat.therm"),
     ("dme/dme_24_mech.txt", "dme/dme_24_therm.txt"),
     ("n-heptane_reduced/heptanesymp159_mec.txt", "n-heptane_reduced/heptanesymp_therm.txt"),
+    ("plog/plog_test.mech", "plog/plog_test.therm"),
+    ("ideal/plog_test.mech", "ideal/const_specific_heat.therm"),
 ])
 def test_oracle_matches_reference_library(mech, therm):
     m, t = os.path.join(REF_DATA, mech), os.path.join(REF_DATA, therm)
@@ -223,3 +225,44 @@ def test_troe_known_answer(tmp_path):
         F = 10 ** (f / (1 + lp * lp))
         expect = 2.0e12 * F * Pr / (1 + Pr)
         assert abs(K[rxn] - expect) <= 6e-15 * abs(expect)
+
+
+def test_plog_known_answers():
+    """PLOG rate coefficients of data/mechanisms/ideal/plog_test.mech against
+    the closed forms of the reference's tests/reactions/plog_gtest.cpp (6e-15
+    relative there): single-pressure tables (positive, negative and summed
+    duplicate lines) give A T^2 exp(-1000 K / T) at every pressure, and a
+    three-pressure table with duplicate lines interpolates log-linearly in
+    pressure and stays flat outside its range.  Product loader tables, oracle
+    evaluation (committed fixture copy of the mechanism).  Tolerance 2e-14
+    relative (the gtest's 6e-15 with room for the closed form's own
+    rounding)."""
+    import zerork_b200 as zb
+    from plugin_cases import mech_path
+    pm = zb.Mechanism(mech_path("plog_test_ideal.mech"), mech_path("const_specific_heat.therm"),
+                      device=False)
+    ot = oracle_tables(pm)
+    steps = pm.table("step_rxn")
+    fwd = [int(np.nonzero((steps == j) & (pm.table("step_dir") == 1))[0][0]) for j in range(pm.nrxn)]
+    ru, patm = 8.314462618e3, 1.01325e5
+
+    def kf(T, p_atm):
+        P = p_atm * patm
+        c = np.full(pm.nsp, P / (ru * T) / pm.nsp)
+        return ot.rate_coefs(T, c)
+
+    def near(a, b):  # the closed form's own rounding (Ta = 1000 K up to 1 ulp) needs 2e-14
+        return abs(a - b) <= 2e-14 * max(abs(a), abs(b))
+
+    for T in (300.0, 1000.0, 2500.0):
+        base = 1.0e6 * T ** 2 * math.exp(-1000.0 / T)
+        for p in (0.1, 1.0, 10.0):
+            K = kf(T, p)
+            assert near(K[fwd[0]], base) and near(K[fwd[1]], -base)
+            assert near(K[fwd[2]], 0.9 * base)
+        # duplicates summed per pressure: 6.2 at 1 atm, 1.3 at 2 atm, 10.01 at 4 atm
+        # (cgs A / 1000 for a second-order step); flat outside [1, 4] atm
+        K = kf(T, 1.5)
+        want = 6.2 * 1.5 ** (math.log(1.3 / 6.2) / math.log(2.0))
+        assert abs(K[fwd[5]] - want) <= 1e-13 * want
+        assert near(kf(T, 0.5)[fwd[5]], 6.2) and near(kf(T, 8.0)[fwd[5]], 10.01)

@@ -80,7 +80,9 @@ def measure_fp64():
 TABLE_NAMES = ("mw", "thermo", "step_rxn", "step_dir", "reac_ptr", "reac_spc", "prod_ptr",
                "prod_spc", "arr_step", "arr_lnA", "arr_n", "arr_Ta", "keq_step", "keq_fwd",
                "keq_dn", "tb_fwd", "tb_rev", "tb_ptr", "tb_spc", "tb_alpha", "fo_fwd", "fo_rev",
-               "fo_type", "fo_spc", "fo_ptr", "fo_eff_spc", "fo_alpha", "fo_par")
+               "fo_type", "fo_spc", "fo_ptr", "fo_eff_spc", "fo_alpha", "fo_par", "plog_step",
+               "plog_pt_ptr", "plog_ln_ptr", "plog_p", "plog_lnp", "plog_lnA", "plog_sgn", "plog_n",
+               "plog_Ta")
 
 
 class Mechanism:

@@ -157,6 +157,8 @@ int zrk_mech_table(zrk_mech_t m, const char *name, void *out, long capacity, lon
   TI(arr_step) TD(arr_lnA) TD(arr_n) TD(arr_Ta) TI(keq_step) TI(keq_fwd) TD(keq_dn)
   TI(tb_fwd) TI(tb_rev) TI(tb_ptr) TI(tb_spc) TD(tb_alpha)
   TI(fo_fwd) TI(fo_rev) TI(fo_type) TI(fo_spc) TI(fo_ptr) TI(fo_eff_spc) TD(fo_alpha) TD(fo_par)
+  TI(plog_step) TI(plog_pt_ptr) TI(plog_ln_ptr) TD(plog_p) TD(plog_lnp) TD(plog_lnA) TD(plog_sgn)
+  TD(plog_n) TD(plog_Ta)
 #undef TI
 #undef TD
   if (!vi && !vd) return set_error(ZRK_ERR_INVALID_ARGUMENT, "unknown table " + n);

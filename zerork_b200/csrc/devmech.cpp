@@ -41,6 +41,8 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   std::vector<RxnRec> rec(t.nrxn);
   std::vector<int> arr_of_step(t.nstep, -1);
   for (size_t k = 0; k < t.arr_step.size(); ++k) arr_of_step[t.arr_step[k]] = (int)k;
+  std::vector<int> plog_of_step(t.nstep, -1);
+  for (size_t k = 0; k < t.plog_step.size(); ++k) plog_of_step[t.plog_step[k]] = (int)k;
   std::vector<int> step_of_fwd(t.nrxn, -1), step_of_rev(t.nrxn, -1);
   for (int s = 0; s < t.nstep; ++s) {
     if (t.step_dir[s] == 1) step_of_fwd[t.step_rxn[s]] = s;
@@ -51,11 +53,18 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
     std::memset(&R, 0, sizeof(R));
     R.fwd = step_of_fwd[j];
     R.rev = step_of_rev[j];
+    R.aux = -1;
     int a = arr_of_step[R.fwd];
-    if (a < 0) throw std::runtime_error("forward step without Arrhenius parameters");
-    R.lnA = t.arr_lnA[a];
-    R.n = t.arr_n[a];
-    R.Ta = t.arr_Ta[a];
+    if (a >= 0) {
+      R.lnA = t.arr_lnA[a];
+      R.n = t.arr_n[a];
+      R.Ta = t.arr_Ta[a];
+    } else if (plog_of_step[R.fwd] >= 0) {
+      R.flags |= kPlog;
+      R.aux = plog_of_step[R.fwd];
+    } else {
+      throw std::runtime_error("forward step without Arrhenius or PLOG parameters");
+    }
     if (R.rev >= 0) {
       int b = arr_of_step[R.rev];
       if (b >= 0) {
@@ -73,7 +82,6 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
       throw std::runtime_error("reaction " + std::to_string(j) + " has more than 6 species on a side");
     for (int k = 0; k < R.nr; ++k) R.r[k] = (short)t.reac_spc[t.reac_ptr[R.fwd] + k];
     for (int k = 0; k < R.np; ++k) R.p[k] = (short)t.prod_spc[t.prod_ptr[R.fwd] + k];
-    R.aux = -1;
   }
   for (size_t k = 0; k < t.keq_step.size(); ++k) {
     int j = t.step_rxn[t.keq_fwd[k]];
@@ -141,6 +149,10 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
     if (R.flags & (kRevKeq | kRevArr)) c += 1.0;
     if (R.flags & kThirdBody) c += 0.5 + 0.1 * (t.tb_ptr[R.aux + 1] - t.tb_ptr[R.aux]);
     if (R.flags & kFalloff) c += 3.0 + 0.1 * (t.fo_ptr[R.aux + 1] - t.fo_ptr[R.aux]);
+    if (R.flags & kPlog) {
+      const int q0 = t.plog_pt_ptr[R.aux], q1 = t.plog_pt_ptr[R.aux + 1];
+      c += 2.0 + 0.5 * (t.plog_ln_ptr[q1] - t.plog_ln_ptr[q0]);
+    }
     rc[j] = c;
   }
   for (int k = 0; k < ns; ++k) {
@@ -158,6 +170,9 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   size_t o_tbp = b.add(t.tb_ptr), o_tbs = b.add(t.tb_spc), o_tba = b.add(t.tb_alpha);
   size_t o_fop = b.add(t.fo_ptr), o_foe = b.add(t.fo_eff_spc), o_fot = b.add(t.fo_type),
          o_fos = b.add(t.fo_spc), o_foa = b.add(t.fo_alpha), o_fopar = b.add(t.fo_par);
+  size_t o_plpp = b.add(t.plog_pt_ptr), o_pllp = b.add(t.plog_ln_ptr), o_plp = b.add(t.plog_p),
+         o_pllnp = b.add(t.plog_lnp), o_pla = b.add(t.plog_lnA), o_pls = b.add(t.plog_sgn),
+         o_pln = b.add(t.plog_n), o_plt = b.add(t.plog_Ta);
   size_t o_sdp = b.add(sd_ptr), o_sds = b.add(sd_step), o_scp = b.add(sc_ptr), o_scs = b.add(sc_step);
   size_t o_cp = b.add(p.col_ptr), o_ri = b.add(p.row_idx), o_lr = b.add(p.last_row);
   size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
@@ -185,6 +200,14 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   view_.fo_spc = (const int *)P(o_fos);
   view_.fo_alpha = (const double *)P(o_foa);
   view_.fo_par = (const double *)P(o_fopar);
+  view_.plog_pt_ptr = (const int *)P(o_plpp);
+  view_.plog_ln_ptr = (const int *)P(o_pllp);
+  view_.plog_p = (const double *)P(o_plp);
+  view_.plog_lnp = (const double *)P(o_pllnp);
+  view_.plog_lnA = (const double *)P(o_pla);
+  view_.plog_sgn = (const double *)P(o_pls);
+  view_.plog_n = (const double *)P(o_pln);
+  view_.plog_Ta = (const double *)P(o_plt);
   view_.sd_ptr = (const int *)P(o_sdp);
   view_.sd_step = (const int *)P(o_sds);
   view_.sc_ptr = (const int *)P(o_scp);

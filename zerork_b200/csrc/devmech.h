@@ -23,6 +23,7 @@ enum RxnFlags : int {
   kRevArr = 2,       // reverse step from explicit REV parameters
   kThirdBody = 4,
   kFalloff = 8,
+  kPlog = 16,        // forward rate from the PLOG table (aux: PLOG index)
 };
 
 struct alignas(16) RxnRec {
@@ -45,6 +46,10 @@ struct DevMech {
   const double *tb_alpha;
   const int *fo_ptr, *fo_spc_eff, *fo_type, *fo_spc;
   const double *fo_alpha, *fo_par;
+  // PLOG reactions: distinct pressures per reaction (plog_pt_ptr), Arrhenius
+  // lines per pressure (plog_ln_ptr); see MechTables
+  const int *plog_pt_ptr, *plog_ln_ptr;
+  const double *plog_p, *plog_lnp, *plog_lnA, *plog_sgn, *plog_n, *plog_Ta;
   // species production gather lists (step indices in ascending step order)
   const int *sd_ptr, *sd_step, *sc_ptr, *sc_step;
   // Jacobian pattern and per-nonzero gather lists

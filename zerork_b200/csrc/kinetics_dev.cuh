@@ -39,6 +39,35 @@ __device__ __forceinline__ double nasa_cp(const double *__restrict__ c, double T
   return c[o] + T * (c[o + 1] + T * (c[o + 2] + T * (c[o + 3] + T * c[o + 4])));
 }
 
+// A PLOG reaction's forward rate coefficient at (T, P): the Arrhenius lines
+// of each distinct pressure summed with the sign of their A, the end
+// pressures' values outside [p_min, p_max] and logarithmic interpolation
+// between the bracketing pressures inside; zero for T or P <= 0 or a
+// non-positive bracketing value (src/zerork/plog_reaction.cpp:166-300,
+// without extrapolation as rate_const.cpp:1174-1182 builds them).
+__device__ __forceinline__ double plog_at(const DevMech &m, int q, double invT, double logT) {
+  double k = 0.0;
+  for (int l = m.plog_ln_ptr[q]; l < m.plog_ln_ptr[q + 1]; ++l)
+    k += m.plog_sgn[l] * exp(m.plog_lnA[l] + logT * m.plog_n[l] - invT * m.plog_Ta[l]);
+  return k;
+}
+
+static __device__ __noinline__ double plog_rate(const DevMech &m, int j, double T, double invT, double logT,
+                                         double P) {
+  const int q0 = m.plog_pt_ptr[j], q1 = m.plog_pt_ptr[j + 1];
+  if (T <= 0.0 || P <= 0.0) return 0.0;
+  if (q1 - q0 == 1 || P <= m.plog_p[q0]) return plog_at(m, q0, invT, logT);
+  if (P >= m.plog_p[q1 - 1]) return plog_at(m, q1 - 1, invT, logT);
+  int r = q0;
+  while (r + 1 < q1 - 1 && !(m.plog_p[r] <= P && P < m.plog_p[r + 1])) ++r;
+  const double k1 = plog_at(m, r, invT, logT);
+  if (k1 <= 0.0) return 0.0;
+  const double k2 = plog_at(m, r + 1, invT, logT);
+  if (k2 <= 0.0) return 0.0;
+  const double e = log(k2 / k1) / (m.plog_lnp[r + 1] - m.plog_lnp[r]);
+  return k1 * pow(P / m.plog_p[r], e);
+}
+
 // One reaction (both steps) for the V states a thread owns (states
 // q + k*GS of the tile): rate constants, third body, falloff, step limiter
 // and concentration products.  The V independent chains give the scheduler
@@ -52,8 +81,13 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
                                               const double *Csum, double lim) {
   constexpr int GS = TS / V;
   double kf[V], kr[V];
+  if (R.flags & kPlog) {  // at the pressure of the concentrations, Csum Ru T (rate_const.cpp:548-567)
 #pragma unroll
-  for (int k = 0; k < V; ++k) kf[k] = exp(R.lnA + R.n * logT[k] - R.Ta * invT[k]);
+    for (int k = 0; k < V; ++k) kf[k] = plog_rate(m, R.aux, T[k], invT[k], logT[k], Csum[k] * kRuD * T[k]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; ++k) kf[k] = exp(R.lnA + R.n * logT[k] - R.Ta * invT[k]);
+  }
   if (R.flags & kRevArr) {
 #pragma unroll
     for (int k = 0; k < V; ++k) kr[k] = exp(R.lnA_r + R.n_r * logT[k] - R.Ta_r * invT[k]);

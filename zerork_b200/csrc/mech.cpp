@@ -3,12 +3,13 @@
 // Supported: ELEMENTS, SPECIES, THERMO (in the mechanism or thermo file),
 // REACTIONS with CAL/MOLE, KCAL/MOLE, JOULES/MOLE, KJOULES/MOLE, KELVINS and
 // MOLES units; elementary, +M third-body and (+M)/(+species) falloff
-// reactions with LOW, TROE (3/4 parameters), SRI (3/5 parameters), REV, DUP
-// and collision efficiencies.  PLOG, FORD/RORD, HIGH and Landau-Teller
+// reactions with LOW, TROE (3/4 parameters), SRI (3/5 parameters), REV, DUP,
+// PLOG and collision efficiencies.  FORD/RORD, HIGH and Landau-Teller
 // reactions, and non-integer stoichiometry, are rejected with a ParseError.
 #include "mech.h"
 
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <cmath>
 #include <cstdlib>
@@ -27,6 +28,7 @@ const double kKcalPerMolTact = 4184.0 / kRu * 1000.0;
 const double kKjoulesPerMolTact = 238.846 * kCalPerMolTact;
 const double kJoulesPerMolTact = 238.846 * kCalPerMolTact / 1000.0;
 const double kConvertC = 1000.0;  // mol/cm^3 -> kmol/m^3
+const double kPatm = 1.01325e5;   // src/zerork/constants.h:12
 const double kArrheniusRtol = 1.0e-6;
 
 // IUPAC 2007 standard atomic weights [kg/kmol] (the table Zero-RK uses,
@@ -204,6 +206,7 @@ struct Reaction {
   int ftype = kLindemann;
   std::vector<double> fpar;
   std::map<std::string, double> e3b;  // std::map: efficiency order by name
+  std::vector<std::array<double, 4>> plog;  // PLOG lines: p [atm], A, n, E
   int line = 0;
 };
 
@@ -342,7 +345,8 @@ MechTables load_chemkin(const std::string &mech_file, const std::string &therm_f
           R.kf.A = num_or_throw(tk[tk.size() - 3], "A");
           R.kf.n = num_or_throw(tk[tk.size() - 2], "n");
           R.kf.E = num_or_throw(tk[tk.size() - 1], "E");
-          if (R.kf.A < 0.0) throw ParseError("negative prefactor at line " + std::to_string(R.line));
+          // a negative A is kept: only a PLOG reaction may carry one (its
+          // lines replace the rate), checked when the reaction is complete
           std::string rs;
           for (size_t k = 0; k + 3 < tk.size(); ++k) rs += tk[k];
           m = rs.find("(+");
@@ -421,8 +425,12 @@ MechTables load_chemkin(const std::string &mech_file, const std::string &therm_f
             R.krev.E = num_or_throw(dt[2], "REV");
           } else if (u.compare(0, 3, "DUP") == 0) {
             // duplicate marker: no effect on the tables
-          } else if (u == "PLOG" || u == "FORD" || u == "RORD" || u == "HIGH" || u == "LT" ||
-                     u == "RLT") {
+          } else if (u == "PLOG") {  // CKParser.cpp:1642-1660: p [atm], A, n, E
+            if (dt.size() != 4) throw ParseError("expected 4 PLOG parameters at line " + std::to_string(L[i].no));
+            std::array<double, 4> v;
+            for (int q = 0; q < 4; ++q) v[q] = num_or_throw(dt[q], "PLOG");
+            R.plog.push_back(v);
+          } else if (u == "FORD" || u == "RORD" || u == "HIGH" || u == "LT" || u == "RLT") {
             throw ParseError(u + " reactions are not supported by this build");
           } else if (!name.empty()) {
             bool is_sp = false;
@@ -477,6 +485,18 @@ MechTables load_chemkin(const std::string &mech_file, const std::string &therm_f
   for (auto &q : sp)
     if (!q.have) throw ParseError("no thermo data for species " + q.name);
 
+  // PLOG reactions exclude falloff, third-body and REV data (CKParser.cpp:
+  // 312-350); other reactions need a non-negative prefactor
+  for (auto &R : rx) {
+    if (R.plog.empty()) {
+      if (R.kf.A < 0.0) throw ParseError("negative prefactor at line " + std::to_string(R.line));
+      continue;
+    }
+    if (R.falloff || R.have_low) throw ParseError("PLOG and falloff are exclusive at line " + std::to_string(R.line));
+    if (R.third_body) throw ParseError("PLOG and third-body are exclusive at line " + std::to_string(R.line));
+    if (R.krev.A > -1.0e299) throw ParseError("PLOG does not take REV at line " + std::to_string(R.line));
+  }
+
   // ---- species tables
   t.nsp = (int)sp.size();
   std::map<std::string, int> idx;
@@ -514,6 +534,7 @@ MechTables load_chemkin(const std::string &mech_file, const std::string &therm_f
     t.rxn_reversible.push_back(rev ? 1 : 0);
     t.rxn_third_body.push_back(R.third_body ? 1 : 0);
     t.rxn_falloff.push_back(R.falloff ? 1 : 0);
+    t.rxn_plog.push_back(R.plog.empty() ? 0 : 1);
     fwd_of[j] = (int)t.step_rxn.size();
     t.step_rxn.push_back(j);
     t.step_dir.push_back(1);
@@ -543,8 +564,11 @@ MechTables load_chemkin(const std::string &mech_file, const std::string &therm_f
   for (int s = 0; s < t.nstep; ++s) {
     const Reaction &R = rx[t.step_rxn[s]];
     const RCoef *k = nullptr;
-    if (t.step_dir[s] == 1) k = &R.kf;
-    else if (R.krev.A > 0.0) k = &R.krev;
+    if (t.step_dir[s] == 1) {
+      if (R.plog.empty()) k = &R.kf;  // PLOG steps have their own list
+    } else if (R.krev.A > 0.0) {
+      k = &R.krev;
+    }
     if (!k) continue;
     AE e;
     e.step = s;
@@ -598,6 +622,46 @@ MechTables load_chemkin(const std::string &mech_file, const std::string &therm_f
       t.keq_dn.push_back((double)((t.prod_ptr[f + 1] - t.prod_ptr[f]) - (t.reac_ptr[f + 1] - t.reac_ptr[f])));
     }
   }
+
+  // ---- PLOG reactions (rate_const.cpp:1146-1185, plog_reaction.cpp:8-132):
+  // pressure [atm] -> Pa, E -> K, A * convertC^(1 - order); lines sorted by
+  // pressure (selection sort: the first strict minimum of the rest swaps in),
+  // then grouped into distinct pressures at relative tolerance 1e-8
+  t.plog_pt_ptr.push_back(0);
+  t.plog_ln_ptr.push_back(0);
+  for (int j = 0; j < t.nrxn; ++j) {
+    const Reaction &R = rx[j];
+    if (R.plog.empty()) continue;
+    const int f = fwd_of[j];
+    t.plog_step.push_back(f);
+    std::vector<std::array<double, 5>> ln;  // p, ln|A|, sign, n, Ta
+    for (auto &v : R.plog) {
+      const double A = v[1] * std::pow(kConvertC, (1.0 - order(f)));
+      ln.push_back({v[0] * kPatm, std::log(std::fabs(A)), (A < 0.0) ? -1.0 : 1.0, v[2], v[3] * convertE});
+    }
+    for (size_t a = 0; a + 1 < ln.size(); ++a) {
+      size_t mi = a;
+      for (size_t b = a + 1; b < ln.size(); ++b)
+        if (ln[b][0] < ln[mi][0]) mi = b;
+      if (mi != a) std::swap(ln[a], ln[mi]);
+    }
+    double last = ln[0][0];
+    t.plog_p.push_back(last);
+    for (size_t a = 0; a < ln.size(); ++a) {
+      if (a > 0 && std::fabs(ln[a][0] - last) > std::fabs(last * 1.0e-8)) {
+        t.plog_ln_ptr.push_back((int)t.plog_lnA.size());
+        last = ln[a][0];
+        t.plog_p.push_back(last);
+      }
+      t.plog_lnA.push_back(ln[a][1]);
+      t.plog_sgn.push_back(ln[a][2]);
+      t.plog_n.push_back(ln[a][3]);
+      t.plog_Ta.push_back(ln[a][4]);
+    }
+    t.plog_ln_ptr.push_back((int)t.plog_lnA.size());
+    t.plog_pt_ptr.push_back((int)t.plog_p.size());
+  }
+  for (double p : t.plog_p) t.plog_lnp.push_back(std::log(p));
 
   // ---- third-body and falloff lists
   t.tb_ptr.push_back(0);

@@ -34,7 +34,13 @@ struct MechTables {
   std::vector<double> tb_alpha;
   std::vector<int> fo_fwd, fo_rev, fo_type, fo_spc, fo_ptr, fo_eff_spc;
   std::vector<double> fo_alpha, fo_par;  // fo_par: 8 per falloff reaction
-  std::vector<int> rxn_reversible, rxn_third_body, rxn_falloff;
+  // PLOG reactions (src/zerork/plog_reaction.cpp, rate_const.cpp:1146-1201):
+  // forward step, distinct pressure points (Pa, ascending, with their logs)
+  // [plog_pt_ptr[j], plog_pt_ptr[j+1]), and per point the Arrhenius lines
+  // [plog_ln_ptr[q], plog_ln_ptr[q+1]) summed with the sign of their A
+  std::vector<int> plog_step, plog_pt_ptr, plog_ln_ptr;
+  std::vector<double> plog_p, plog_lnp, plog_lnA, plog_sgn, plog_n, plog_Ta;
+  std::vector<int> rxn_reversible, rxn_third_body, rxn_falloff, rxn_plog;
 
   int tot_reac() const { return (int)reac_spc.size(); }
   int tot_prod() const { return (int)prod_spc.size(); }
