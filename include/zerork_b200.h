@@ -122,6 +122,28 @@ int zrk_rates_jac_dev_noalloc(zrk_mech_t m, int n, int ld, const double *T, cons
                               const double *Y, double *wdot, double *jac, double *ydot,
                               void *stream);
 
+/* Rates from temperature and concentrations for n independent states:
+ * mechanism_cuda::getReactionRates_CUDA_mr_dev and
+ * getReactionRatesLimiter_CUDA_mr_dev (src/zerork/mechanism_cuda.h:19-26,
+ * perf_net.cpp:126-274 per state).  Device arrays, species-major with
+ * leading dimension ld: T[ld], C[nsp][ld] (kmol/m^3); outputs net, create,
+ * destroy [nsp][ld] and rop [nstep][ld] (rates of progress per step); any
+ * output may be NULL.  step_limiter: one limit per step [nstep] (a step is
+ * limited as K L / (L + K) when 0 < L < 1e300), or NULL for the unlimited
+ * rates of getReactionRates.  T is used as given; PLOG reactions see the
+ * pressure Csum Ru T.  Asynchronous on stream. */
+int zrk_rates_tc_dev(zrk_mech_t m, int n, int ld, const double *T, const double *C,
+                     const double *step_limiter, double *net, double *create, double *destroy,
+                     double *rop, void *stream);
+
+/* The same with host arrays (species-major, ld = n; for one state simply
+ * C[nsp], net[nsp], rop[nstep]): the host-side mechanism::getReactionRates /
+ * getNetReactionRates / getReactionRatesLimiter (src/zerork/mechanism.h:
+ * 114-143).  Copies in, computes on the GPU, copies out, synchronizes. */
+int zrk_rates_tc_host(zrk_mech_t m, int n, const double *T, const double *C,
+                      const double *step_limiter, double *net, double *create, double *destroy,
+                      double *rop);
+
 /* Same with host buffers (species-major, ld = n): copies in, computes,
  * copies out, synchronizes.  Host buffers may be pageable or pinned. */
 int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, const double *Y,

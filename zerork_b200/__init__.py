@@ -50,6 +50,8 @@ def lib():
                                         C.POINTER(C.c_float)]
         L.zrk_rates_jac_dev.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp]
         L.zrk_rates_jac_host.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
+        L.zrk_rates_tc_dev.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
+        L.zrk_rates_tc_host.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
         L.zrk_measure_fp64.argtypes = [dp, dp]
         _lib = L
     return _lib
@@ -173,6 +175,36 @@ class Mechanism:
         s = None if stream is None else C.c_void_p(stream)
         check(lib().zrk_rates_jac_dev(self._h, n, ld, _ptr(T), _ptr(P), _ptr(Y), _ptr(wdot),
                                       _ptr(jac), _ptr(ydot), s))
+
+    def rates_tc(self, T, conc, step_limiter=None, stream=None):
+        """Rates from temperature and concentrations (mechanism_cuda's
+        getReactionRates(Limiter)_CUDA_mr_dev): device tensors T[n],
+        C[nsp, n] (species-major); returns device tensors (net, create,
+        destroy [nsp, n], rop [nstep, n])."""
+        import torch
+        n = T.shape[0]
+        ld = conc.shape[1]
+        kw = dict(dtype=torch.float64, device=conc.device)
+        net, cre, des = (torch.empty((self.nsp, ld), **kw) for _ in range(3))
+        rop = torch.empty((self.nstep, ld), **kw)
+        s = None if stream is None else C.c_void_p(stream)
+        check(lib().zrk_rates_tc_dev(self._h, n, ld, _ptr(T), _ptr(conc), _ptr(step_limiter), _ptr(net),
+                                     _ptr(cre), _ptr(des), _ptr(rop), s))
+        return net, cre, des, rop
+
+    def rates_tc_host(self, T, conc, step_limiter=None):
+        """Host arrays T[n], C[nsp, n] (species-major); the host-side
+        getReactionRates(Limiter) for n states.  Returns numpy (net, create,
+        destroy, rop)."""
+        T = np.ascontiguousarray(T, dtype=np.float64).reshape(-1)
+        n = T.shape[0]
+        Cm = np.ascontiguousarray(conc, dtype=np.float64).reshape(self.nsp, n)
+        lim = None if step_limiter is None else np.ascontiguousarray(step_limiter, dtype=np.float64)
+        net, cre, des = (np.zeros((self.nsp, n)) for _ in range(3))
+        rop = np.zeros((self.nstep, n))
+        check(lib().zrk_rates_tc_host(self._h, n, _ptr(T), _ptr(Cm), _ptr(lim), _ptr(net), _ptr(cre),
+                                      _ptr(des), _ptr(rop)))
+        return net, cre, des, rop
 
     def rates_jac_host(self, T, P, Y, want_jac=True):
         """Host numpy arrays (species-major Y[nsp, n]); returns (wdot, jac)."""

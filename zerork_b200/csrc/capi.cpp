@@ -327,6 +327,72 @@ int zrk_rates_jac_dev(zrk_mech_t m, int n, int ld, const double *T, const double
   return ZRK_OK;
 }
 
+int zrk_rates_tc_dev(zrk_mech_t m, int n, int ld, const double *T, const double *C,
+                     const double *step_limiter, double *net, double *create, double *destroy,
+                     double *rop, void *stream) {
+  if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
+  if (n < 0 || ld < n) return set_error(ZRK_ERR_INVALID_ARGUMENT, "need 0 <= n <= ld");
+  if (n == 0) return ZRK_OK;
+  if (!T || !C) return set_error(ZRK_ERR_INVALID_POINTER, "null array");
+  MechHandle *h = reinterpret_cast<MechHandle *>(m);
+  if (!h->dev) return set_error(ZRK_ERR_NO_DEVICE, "handle has no device tables (zrk_mech_parse)");
+  RatesTCArgs a;
+  a.n = n;
+  a.ld = ld;
+  a.T = T;
+  a.C = C;
+  a.lim_step = step_limiter;
+  a.net = net;
+  a.create = create;
+  a.destroy = destroy;
+  a.rop = rop;
+  cudaError_t e = launch_rates_tc(h->dev->view(), a, (cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_error(e, "rates_tc launch");
+  return ZRK_OK;
+}
+
+int zrk_rates_tc_host(zrk_mech_t m, int n, const double *T, const double *C,
+                      const double *step_limiter, double *net, double *create, double *destroy,
+                      double *rop) {
+  if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
+  if (n < 0) return set_error(ZRK_ERR_INVALID_ARGUMENT, "n < 0");
+  if (n == 0) return ZRK_OK;
+  if (!T || !C) return set_error(ZRK_ERR_INVALID_POINTER, "null array");
+  MechHandle *h = reinterpret_cast<MechHandle *>(m);
+  if (!h->dev) return set_error(ZRK_ERR_NO_DEVICE, "handle has no device tables (zrk_mech_parse)");
+  const size_t S = h->tables.nsp, N = h->tables.nstep, dp = sizeof(double);
+  // device slot: T | C | limiter | net | create | destroy | rop
+  const size_t doubles = n + S * n + N + 3 * S * n + N * n;
+  cudaError_t e = h->ensure_pipe(doubles * dp);
+  if (e != cudaSuccess) return cuda_error(e, "device buffers");
+  double *dT = (double *)h->pipe, *dC = dT + n, *dL = dC + S * n, *dN = dL + N, *dCr = dN + S * n,
+         *dDe = dCr + S * n, *dR = dDe + S * n;
+  cudaStream_t st = h->pipe_stream[0];
+  if ((e = cudaMemcpyAsync(dT, T, n * dp, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dC, C, S * n * dp, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+      (step_limiter &&
+       (e = cudaMemcpyAsync(dL, step_limiter, N * dp, cudaMemcpyHostToDevice, st)) != cudaSuccess))
+    return cuda_error(e, "copy in");
+  RatesTCArgs a;
+  a.n = n;
+  a.ld = n;
+  a.T = dT;
+  a.C = dC;
+  a.lim_step = step_limiter ? dL : nullptr;
+  a.net = net ? dN : nullptr;
+  a.create = create ? dCr : nullptr;
+  a.destroy = destroy ? dDe : nullptr;
+  a.rop = rop ? dR : nullptr;
+  if ((e = launch_rates_tc(h->dev->view(), a, st)) != cudaSuccess) return cuda_error(e, "rates_tc launch");
+  if ((net && (e = cudaMemcpyAsync(net, dN, S * n * dp, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+      (create && (e = cudaMemcpyAsync(create, dCr, S * n * dp, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+      (destroy && (e = cudaMemcpyAsync(destroy, dDe, S * n * dp, cudaMemcpyDeviceToHost, st)) != cudaSuccess) ||
+      (rop && (e = cudaMemcpyAsync(rop, dR, N * n * dp, cudaMemcpyDeviceToHost, st)) != cudaSuccess))
+    return cuda_error(e, "copy out");
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_error(e, "rates_tc");
+  return ZRK_OK;
+}
+
 int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, const double *Y,
                        double *wdot, double *jac) {
   if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");

@@ -123,6 +123,23 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
     nzc_ptr.push_back((int)nzc_step.size());
   }
   n_terms_ = (int)(nzd_step.size() + nzc_step.size());
+  // flat species-column list for the rates kernel's Jacobian phase
+  std::vector<int2> jw;
+  std::vector<unsigned short> jt;
+  std::vector<int> jt_ptr(1, 0), jcost(1, 0), jf_ptr(1, 0);
+  for (int j = 0; j < ns; ++j) {
+    for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1] - 1; ++k) {  // the last entry is the T row
+      const int nd = nzd_ptr[k + 1] - nzd_ptr[k], nc = nzc_ptr[k + 1] - nzc_ptr[k];
+      if (nd > 0xffff || nc > 0xffff || t.nstep > 0xffff)
+        throw std::runtime_error("mechanism too large for 16-bit Jacobian term lists");
+      jw.push_back(make_int2(p.row_idx[k], nd | (nc << 16)));
+      for (int q = nzd_ptr[k]; q < nzd_ptr[k + 1]; ++q) jt.push_back((unsigned short)nzd_step[q]);
+      for (int q = nzc_ptr[k]; q < nzc_ptr[k + 1]; ++q) jt.push_back((unsigned short)nzc_step[q]);
+      jt_ptr.push_back((int)jt.size());
+      jcost.push_back(jcost.back() + 3 + nd + nc);
+    }
+    jf_ptr.push_back((int)jw.size());
+  }
   std::vector<std::vector<std::pair<int, int>>> rows(p.n);
   for (int j = 0; j < p.n; ++j)
     for (int k = p.col_ptr[j]; k < p.col_ptr[j + 1]; ++k) rows[p.row_idx[k]].push_back({k, j});
@@ -177,6 +194,8 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   size_t o_cp = b.add(p.col_ptr), o_ri = b.add(p.row_idx), o_lr = b.add(p.last_row);
   size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
   size_t o_jrp = b.add(jr_ptr), o_jrk = b.add(jr_kk), o_jrc = b.add(jr_col);
+  size_t o_jw = b.add(jw), o_jt = b.add(jt), o_jtp = b.add(jt_ptr), o_jc = b.add(jcost),
+         o_jf = b.add(jf_ptr);
   size_t o_ro = b.add(rxn_order), o_so = b.add(spc_order), o_co = b.add(col_order);
   bytes_ = b.bytes.size();
   check(cudaMalloc(&blob_, bytes_), "cudaMalloc(mechanism tables)");
@@ -219,6 +238,12 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   view_.nzd_step = (const int *)P(o_nds);
   view_.nzc_ptr = (const int *)P(o_ncp);
   view_.nzc_step = (const int *)P(o_ncs);
+  view_.nj = (int)jw.size();
+  view_.jw = (const int2 *)P(o_jw);
+  view_.jt = (const unsigned short *)P(o_jt);
+  view_.jt_ptr = (const int *)P(o_jtp);
+  view_.jcost = (const int *)P(o_jc);
+  view_.jf_ptr = (const int *)P(o_jf);
   view_.jr_ptr = (const int *)P(o_jrp);
   view_.jr_kk = (const int *)P(o_jrk);
   view_.jr_col = (const int *)P(o_jrc);

@@ -9,6 +9,8 @@
 // Species-production and Jacobian phases use gather lists (per species and
 // per Jacobian nonzero) so every sum is deterministic and atomic-free.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <vector>
 
@@ -55,6 +57,17 @@ struct DevMech {
   // Jacobian pattern and per-nonzero gather lists
   const int *col_ptr, *row_idx, *last_row;
   const int *nzd_ptr, *nzd_step, *nzc_ptr, *nzc_step;
+  // Species-column Jacobian entries as one flat list in column-major order
+  // without each column's temperature row (nj items; column j holds items
+  // [jf_ptr[j], jf_ptr[j+1]), and item f is nonzero f + j of the compressed
+  // columns): per item {row, n_des | n_cre << 16}, its destruction then
+  // creation step indices from jt[jt_ptr[f]], and the cumulative work
+  // estimate jcost[f] (3 + n_des + n_cre per item) that splits the list into
+  // equal shares for the thread groups of the rates kernel.
+  int nj;
+  const int2 *jw;
+  const unsigned short *jt;
+  const int *jt_ptr, *jcost, *jf_ptr;
   // row-wise view of the Jacobian pattern: row i has entries jr_kk[p] (index
   // into the compressed-column values) in columns jr_col[p], p in
   // [jr_ptr[i], jr_ptr[i+1])

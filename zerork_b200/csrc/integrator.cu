@@ -96,7 +96,7 @@ __device__ __forceinline__ int rhs_warp(const DevMech &m, const IntegOpts &o, co
   const double Csum = wsum(pc), cv = wsum(pcv);
   __syncwarp();
   for (int r = lane; r < m.nrxn; r += 32)
-    reaction_item<1, 1>(m, m.rxn[r], 0, w.C, w.G, w.ROP, &T, &logT, &invT, &lprt, &Csum, o.lim);
+    reaction_item<1, 1>(m, load_rxn(m.rxn + r), 0, w.C, w.G, w.ROP, &T, &logT, &invT, &lprt, &Csum, o.lim);
   __syncwarp();
   double pe = 0.0;
   for (int s = lane; s < S; s += 32) {

@@ -131,7 +131,7 @@ __device__ __noinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, const 
   for (int rr = 0; rr * nt < m.nrxn; ++rr) {
     const int pos = rr * nt + ((rr & 1) ? nt - 1 - tid : tid);
     if (pos < m.nrxn)
-      reaction_item<1, 1>(m, m.rxn[m.rxn_order[pos]], 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum,
+      reaction_item<1, 1>(m, load_rxn(m.rxn + m.rxn_order[pos]), 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum,
                           o.lim);
   }
   __syncthreads();

@@ -35,20 +35,25 @@ constexpr double kRu = kRuD;
 constexpr double kPatm = kPatmD;
 
 struct Layout {
-  int rC, rU, rX, rG, rROP, rPart, rScal, rows;
+  int rC, rU, rROP, rG, rPart, rStash, rows;
 };
 
-// NG here is the number of warps: one partial-sum row pair per warp.
-__host__ __device__ inline Layout make_layout(int S, int N, int NG) {
+// Workspace rows of TS doubles: concentrations, u/RT (later the perturbed
+// net rates), rates of progress, g/RT, two buffers of per-warp partial sums
+// (NW = warps) and two rows that keep the temperature derivative and heat
+// capacity of the clamped state through the Jacobian phase.  The g/RT and
+// partial rows are contiguous: in the Jacobian phase they hold the
+// per-(group, column) temperature-row partials.  Kept small so the shared
+// memory carve-out leaves L1 room for the mechanism tables.
+__host__ __device__ inline Layout make_layout(int S, int N, int NW) {
   Layout L;
   L.rC = 0;
   L.rU = S;
-  L.rX = 2 * S;
-  L.rG = 3 * S;
-  L.rROP = 4 * S;
-  L.rPart = 4 * S + N;
-  L.rScal = L.rPart + 4 * NG;  // two buffers of two partial rows per warp
-  L.rows = L.rScal;
+  L.rROP = 2 * S;
+  L.rG = 2 * S + N;
+  L.rPart = 3 * S + N;
+  L.rStash = L.rPart + 2 * NW;
+  L.rows = L.rStash + 2;
   return L;
 }
 
@@ -89,8 +94,8 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
   const bool wlead = (threadIdx.x & 31) < GS;  // holds the warp partial
   const Layout L = make_layout(S, N, NW);
   double *ws = gscratch ? gscratch + (size_t)blockIdx.x * ws_doubles : smem_dyn;
-  double *sC = ws + L.rC * TS, *sU = ws + L.rU * TS, *sX = ws + L.rX * TS, *sG = ws + L.rG * TS;
-  double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS;
+  double *sC = ws + L.rC * TS, *sU = ws + L.rU * TS, *sG = ws + L.rG * TS;
+  double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS, *sStash = ws + L.rStash * TS;
 #define PT(a, ww, k) sPart[((a) * NW + (ww)) * TS + q + (k) * GS]
 #define FORV _Pragma("unroll") for (int k = 0; k < V; ++k)
 // Items of a cost-sorted work list in snake order: round r gives group g the
@@ -122,7 +127,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         FORV pa[k] += yload(s, k) * iw;
       }
       FORV pa[k] = warp_group_sum<GS>(pa[k]);
-      if (wlead) FORV PT(2, w, k) = pa[k];  // second buffer: the species pass follows
+      if (wlead) FORV PT(0, w, k) = pa[k];
     }
     __syncthreads();
     // every thread reduces the warp partials of its own states (same order
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     double v[V], Tr[V], logT[V], invT[V], lprt[V], Csum[V], yS[V], cv[V], cvc[V];
     FORV {
       double sum = 0.0;
-      for (int ww = 0; ww < NW; ++ww) sum += PT(2, ww, k);
+      for (int ww = 0; ww < NW; ++ww) sum += PT(0, ww, k);
       const double T = valid[k] ? Tin[st[k]] : 1000.0;
       const double P = valid[k] ? Pin[st[k]] : kPatm;
       yS[k] = T / kp.Tref;
@@ -145,6 +150,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       invT[k] = 1.0 / t;
       lprt[k] = log(kPatm / (kRu * t));
     }
+    __syncthreads();  // the species pass reuses the partial rows
     // ---- species pass at T: C, g/RT, u/RT, partial sums
     int need = 0;
     {
@@ -188,7 +194,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     }
     // ---- reactions at T
     SNAKE(r, m.rxn_order, m.nrxn)
-      reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
+      reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
     __syncthreads();
     // ---- net production rates, energy partial
     {
@@ -225,8 +231,11 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       __syncthreads();  // the next tile reuses the workspace
       continue;
     }
-    // ---- clamped state (reactor_nvector_serial.cpp:629-640), only if needed
+    // ---- clamped state (reactor_nvector_serial.cpp:629-640), only if needed:
+    // the clamped concentrations take the C rows for this pass and the
+    // unclamped ones are written back after it
     if (need) {
+      __syncthreads();  // the energy partials above may still be read
       {
         double pc[V], pcv[V];
         FORV pc[k] = pcv[k] = 0.0;
@@ -236,7 +245,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           FORV {
             const double yc = clamp_mass_fraction(yload(s, k), kp.mmf);
             const double c = (1.0 / v[k]) * iw * yc;
-            sX[s * TS + q + k * GS] = c;
+            sC[s * TS + q + k * GS] = c;
             pc[k] += c;
             pcv[k] += ((nasa_cp(th, Tr[k]) - 1.0) * riw) * yc;
           }
@@ -245,9 +254,9 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           pc[k] = warp_group_sum<GS>(pc[k]);
           pcv[k] = warp_group_sum<GS>(pcv[k]);
         }
-        if (wlead) FORV {  // second buffer: the energy partials may still be read
-          PT(2, w, k) = pc[k];
-          PT(3, w, k) = pcv[k];
+        if (wlead) FORV {
+          PT(0, w, k) = pc[k];
+          PT(1, w, k) = pcv[k];
         }
       }
       __syncthreads();
@@ -256,16 +265,16 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         FORV {
           double cs = 0.0, c2 = 0.0;
           for (int ww = 0; ww < NW; ++ww) {
-            cs += PT(2, ww, k);
-            c2 += PT(3, ww, k);
+            cs += PT(0, ww, k);
+            c2 += PT(1, ww, k);
           }
           Cc[k] = cs;
           cvc[k] = c2;
         }
         SNAKE(r, m.rxn_order, m.nrxn)
-          reaction_item<TS, V>(m, m.rxn[r], q, sX, sG, sROP, Tr, logT, invT, lprt, Cc, kp.lim);
+          reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, Tr, logT, invT, lprt, Cc, kp.lim);
       }
-      __syncthreads();
+      __syncthreads();  // also fences the reads of PT(0), PT(1) above
       {
         double pe[V];
         FORV pe[k] = 0.0;
@@ -278,6 +287,10 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         }
         FORV pe[k] = warp_group_sum<GS>(pe[k]);
         if (wlead) FORV PT(0, w, k) = pe[k];
+        for (int s = g; s < S; s += NG) {  // the unclamped concentrations again
+          const double iw = m.inv_mw[s];
+          FORV sC[s * TS + q + k * GS] = (1.0 / v[k]) * iw * yload(s, k);
+        }
       }
       __syncthreads();
       FORV {
@@ -286,44 +299,118 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         tdc[k] = -es * kRu * yS[k] / cvc[k] + 0.0;
       }
     }
-    // ---- analytic Jacobian columns + temperature row
+    // ---- analytic Jacobian: the species-column entries (the flat item list of
+    // devmech.h) in equal work shares over the groups, the temperature row of
+    // each column from per-(group, column) partial sums kept in the g/RT and
+    // partial rows (free in this phase: S + NGj - 1 <= S + 2 NW slots of TS
+    // doubles)
+    __syncthreads();  // the energy partials are read before the slots reuse them
     {
-      double RuTemp[V], TdC[V], multFact[V];
-      FORV {
-        RuTemp[k] = kRu * yS[k];
-        TdC[k] = tdc[k];
-        multFact[k] = -1.0 / cvc[k];
+      int NGj = NG < S + 1 ? NG : S + 1;
+      if (NGj > 2 * NW + 1) NGj = 2 * NW + 1;
+      const int total = m.jcost[m.nj];
+      double *sTP = sG;
+      auto group_of = [&](int f) { return (int)(((long long)m.jcost[f] * NGj) / total); };
+      // the temperature derivative and heat capacity of the (clamped) state
+      // wait in partial rows for the temperature-row pass (fewer live registers)
+      if (g == 0) FORV {
+        sStash[q + k * GS] = tdc[k];
+        sStash[TS + q + k * GS] = cvc[k];
       }
-      SNAKE(j, m.col_order, S) {
-        const double mwj = m.mw[j], wcol = m.inv_mw[j];
-        const double *th = m.thermo + 16 * j;
-        const double riw = m.ru_inv_mw[j];
-        double t2[V], trow[V];
-        FORV {
-          t2[k] = mwj / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
-          trow[k] = 0.0;
-        }
-        const int k0 = m.col_ptr[j], k1 = m.col_ptr[j + 1] - 1;
-        for (int kk = k0; kk < k1; ++kk) {
-          const int row = m.row_idx[kk];
-          double des[V], cre[V];
-          FORV des[k] = cre[k] = 0.0;
-          gather_rop<TS, V>(sROP, m.nzd_step, m.nzd_ptr[kk], m.nzd_ptr[kk + 1], q, des);
-          gather_rop<TS, V>(sROP, m.nzc_step, m.nzc_ptr[kk], m.nzc_ptr[kk + 1], q, cre);
-          const double conv = m.mw[row] * wcol;
-          FORV {
-            // destruction terms first, then creation (SetupJacobianSparse order)
-            const double val = (0.0 - des[k] * t2[k]) + cre[k] * t2[k];
-            trow[k] += val * sU[row * TS + q + k * GS];
-            if (valid[k]) jac[(size_t)kk * ld + st[k]] = val * conv;
+      if (g < NGj) {
+        auto first_of = [&](int gg) {  // first item f with group_of(f) >= gg
+          const long long thr = (long long)gg * total;
+          int lo = 0, hi = m.nj;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((long long)m.jcost[mid] * NGj >= thr) hi = mid;
+            else lo = mid + 1;
           }
+          return lo;
+        };
+        const int f0 = first_of(g), f1 = first_of(g + 1);
+        if (f0 < f1) {
+          int j = 0, hi = S;  // the column holding f0: jf_ptr[j] <= f0 < jf_ptr[j+1]
+          while (j < hi) {
+            const int mid = (j + hi + 1) >> 1;
+            if (m.jf_ptr[mid] <= f0) j = mid;
+            else hi = mid - 1;
+          }
+          int jend = m.jf_ptr[j + 1];
+          int t = m.jt_ptr[f0];
+          double t2[V], trow[V], wcol = m.inv_mw[j];
+          FORV {
+            t2[k] = m.mw[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
+            trow[k] = 0.0;
+          }
+          for (int f = f0; f < f1; ++f) {
+            while (f == jend) {  // column j ends inside this share
+              FORV sTP[(j + g) * TS + q + k * GS] = trow[k];
+              ++j;
+              jend = m.jf_ptr[j + 1];
+              wcol = m.inv_mw[j];
+              FORV {
+                t2[k] = m.mw[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
+                trow[k] = 0.0;
+              }
+            }
+            const int2 w = m.jw[f];
+            const int row = w.x, nd = w.y & 0xffff, nc = w.y >> 16;
+            double des[V], cre[V];
+            FORV des[k] = cre[k] = 0.0;
+            for (int e = 0; e < nd; ++e) {
+              const double *rp = sROP + m.jt[t + e] * TS + q;
+              FORV des[k] += rp[k * GS];
+            }
+            t += nd;
+            for (int e = 0; e < nc; ++e) {
+              const double *rp = sROP + m.jt[t + e] * TS + q;
+              FORV cre[k] += rp[k * GS];
+            }
+            t += nc;
+            const double conv = m.mw[row] * wcol;
+            FORV {
+              // destruction terms first, then creation (SetupJacobianSparse order)
+              const double val = (0.0 - des[k] * t2[k]) + cre[k] * t2[k];
+              trow[k] += val * sU[row * TS + q + k * GS];
+              if (valid[k]) jac[(size_t)(f + j) * ld + st[k]] = val * conv;
+            }
+          }
+          FORV sTP[(j + g) * TS + q + k * GS] = trow[k];
+        } else if (f0 < m.nj) {
+          // an empty share inside a column (one item's work spans several
+          // shares): its slot of that column holds a zero partial
+          int j = 0, hi = S;
+          while (j < hi) {
+            const int mid = (j + hi + 1) >> 1;
+            if (m.jf_ptr[mid] <= f0) j = mid;
+            else hi = mid - 1;
+          }
+          FORV sTP[(j + g) * TS + q + k * GS] = 0.0;
         }
+      }
+      __syncthreads();
+      // temperature row of column j: the partials of groups group_of(first
+      // item) .. group_of(last item), in group order
+      for (int j = g; j < S; j += NG) {
+        const int g0 = group_of(m.jf_ptr[j]), g1 = group_of(m.jf_ptr[j + 1] - 1);
+        double tp[V];
+        FORV tp[k] = 0.0;
+#pragma unroll 1
+        for (int gg = g0; gg <= g1; ++gg) {
+          const double *pp = sTP + (j + gg) * TS + q;
+          FORV tp[k] += pp[k * GS];
+        }
+        const double *th = m.thermo + 16 * j;
+        const size_t kk = (size_t)(m.jf_ptr[j + 1] + j) * ld;
         FORV {
-          const double cvj = (nasa_cp(th, Tr[k]) - 1.0) * riw;
-          double tr = trow[k] * RuTemp[k];
-          tr += TdC[k] * cvj * mwj;
-          tr *= wcol * multFact[k];
-          if (valid[k]) jac[(size_t)k1 * ld + st[k]] = tr;
+          double Tk = yS[k] * kp.Tref;  // the clamped temperature of this state
+          if (Tk > 1.0e4) Tk = 1.0e4;
+          const double cvj = (nasa_cp(th, Tk) - 1.0) * m.ru_inv_mw[j];
+          double tr = tp[k] * (kRu * yS[k]);
+          tr += sStash[q + k * GS] * cvj * m.mw[j];
+          tr *= m.inv_mw[j] * (-1.0 / sStash[TS + q + k * GS]);
+          if (valid[k]) jac[kk + st[k]] = tr;
         }
       }
     }
@@ -365,7 +452,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       cvp[k] = c2;
     }
     SNAKE(r, m.rxn_order, m.nrxn)
-      reaction_item<TS, V>(m, m.rxn[r], q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
+      reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
     __syncthreads();
     {
       double pe[V];
@@ -377,8 +464,8 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
         FORV {
           const double net = cre[k] - des[k];
-          sX[s * TS + q + k * GS] = net;
           pe[k] += sU[s * TS + q + k * GS] * net * v[k];
+          sU[s * TS + q + k * GS] = net;  // u/RT at T' is not needed again
         }
       }
       FORV pe[k] = warp_group_sum<GS>(pe[k]);
@@ -399,7 +486,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           double d;
           if (row < S) {
             const double mr = m.mw[row];
-            const double f1 = sX[row * TS + q + k * GS] * mr * v[k];
+            const double f1 = sU[row * TS + q + k * GS] * mr * v[k];
             const double f0 = (valid[k] ? wdot[(size_t)row * ld + st[k]] : 0.0) * mr * v[k];
             d = (f1 - f0) * mult[k];
           } else {
@@ -427,6 +514,12 @@ cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams 
   if (!cfg.global_ws) {
     cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes);
+    if (e != cudaSuccess) return e;
+    // the smallest shared-memory carve-out that holds the workspace, so the
+    // rest of the SM's 256 KB stays L1 for the mechanism tables
+    const int pct = (int)((100 * (ws_bytes + 1024) + 228 * 1024 - 1) / (228 * 1024));
+    e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, pct < 100 ? pct : 100);
     if (e != cudaSuccess) return e;
     rates_jac_kernel<TS, V, MAXT><<<ntiles, threads, ws_bytes, stream>>>(
         m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac, a.ydot, kp, nullptr, 0);

@@ -38,6 +38,18 @@ struct RatesJacArgs {
   size_t scratch_bytes = 0;
 };
 
+// Rates from temperature and concentrations (rates_tc.cu): species-major
+// C[nsp][ld], outputs net / create / destroy [nsp][ld] and rates of progress
+// rop [nstep][ld] (any output may be null); lim_step: one limit per step
+// (null: no limiter).
+struct RatesTCArgs {
+  int n = 0, ld = 0;
+  const double *T = nullptr, *C = nullptr, *lim_step = nullptr;
+  double *net = nullptr, *create = nullptr, *destroy = nullptr, *rop = nullptr;
+};
+size_t rates_tc_smem_bytes(const DevMech &m, int ts, int threads);
+cudaError_t launch_rates_tc(const DevMech &m, const RatesTCArgs &a, cudaStream_t stream);
+
 size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg);
 bool rates_jac_mapping_ok(const LaunchCfg &cfg);
 cudaError_t launch_rates_jac(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,

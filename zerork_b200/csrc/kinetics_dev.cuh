@@ -52,7 +52,7 @@ __device__ __forceinline__ double plog_at(const DevMech &m, int q, double invT, 
   return k;
 }
 
-static __device__ __noinline__ double plog_rate(const DevMech &m, int j, double T, double invT, double logT,
+static __device__ __forceinline__ double plog_rate(const DevMech &m, int j, double T, double invT, double logT,
                                          double P) {
   const int q0 = m.plog_pt_ptr[j], q1 = m.plog_pt_ptr[j + 1];
   if (T <= 0.0 || P <= 0.0) return 0.0;
@@ -68,9 +68,23 @@ static __device__ __noinline__ double plog_rate(const DevMech &m, int j, double 
   return k1 * pow(P / m.plog_p[r], e);
 }
 
+// A reaction record read as six independent 16-byte loads: one memory round
+// trip instead of a chain of dependent field loads.
+__device__ __forceinline__ RxnRec load_rxn(const RxnRec *p) {
+  static_assert(sizeof(RxnRec) == 96, "RxnRec layout");
+  const int4 *src = reinterpret_cast<const int4 *>(p);
+  int4 b[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) b[i] = __ldg(src + i);
+  RxnRec R;
+  memcpy(&R, b, sizeof(R));
+  return R;
+}
+
 // One reaction (both steps) for the V states a thread owns (states
 // q + k*GS of the tile): rate constants, third body, falloff, step limiter
-// and concentration products.  The V independent chains give the scheduler
+// (one scalar for all steps, or one per step when lim_step is given) and
+// concentration products.  The V independent chains give the scheduler
 // instruction-level parallelism across states.
 template <int TS, int V>
 __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R, int q,
@@ -78,7 +92,8 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
                                               const double *__restrict__ sG, double *sROP,
                                               const double *T, const double *logT,
                                               const double *invT, const double *lprt,
-                                              const double *Csum, double lim) {
+                                              const double *Csum, double lim,
+                                              const double *lim_step = nullptr) {
   constexpr int GS = TS / V;
   double kf[V], kr[V];
   if (R.flags & kPlog) {  // at the pressure of the concentrations, Csum Ru T (rate_const.cpp:548-567)
@@ -115,7 +130,24 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
     double Cm[V];
 #pragma unroll
     for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
-    for (int e = m.tb_ptr[R.aux]; e < m.tb_ptr[R.aux + 1]; ++e) {
+    // efficiencies four at a time: the table loads are independent of the
+    // sums, which keep the list order
+    const int e0 = m.tb_ptr[R.aux], e1 = m.tb_ptr[R.aux + 1];
+    int e = e0;
+    for (; e + 3 < e1; e += 4) {
+      const double a0 = m.tb_alpha[e], a1 = m.tb_alpha[e + 1], a2 = m.tb_alpha[e + 2],
+                   a3 = m.tb_alpha[e + 3];
+      const double *c0 = sC + m.tb_spc[e] * TS + q, *c1 = sC + m.tb_spc[e + 1] * TS + q,
+                   *c2 = sC + m.tb_spc[e + 2] * TS + q, *c3 = sC + m.tb_spc[e + 3] * TS + q;
+#pragma unroll
+      for (int k = 0; k < V; ++k) {
+        Cm[k] += c0[k * GS] * a0;
+        Cm[k] += c1[k * GS] * a1;
+        Cm[k] += c2[k * GS] * a2;
+        Cm[k] += c3[k * GS] * a3;
+      }
+    }
+    for (; e < e1; ++e) {
       const double a = m.tb_alpha[e];
       const double *cp = sC + m.tb_spc[e] * TS + q;
 #pragma unroll
@@ -139,7 +171,22 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
     } else {
 #pragma unroll
       for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
-      for (int e = m.fo_ptr[f]; e < m.fo_ptr[f + 1]; ++e) {
+      const int e0 = m.fo_ptr[f], e1 = m.fo_ptr[f + 1];
+      int e = e0;
+      for (; e + 3 < e1; e += 4) {
+        const double a0 = m.fo_alpha[e], a1 = m.fo_alpha[e + 1], a2 = m.fo_alpha[e + 2],
+                     a3 = m.fo_alpha[e + 3];
+        const double *c0 = sC + m.fo_spc_eff[e] * TS + q, *c1 = sC + m.fo_spc_eff[e + 1] * TS + q,
+                     *c2 = sC + m.fo_spc_eff[e + 2] * TS + q, *c3 = sC + m.fo_spc_eff[e + 3] * TS + q;
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          Cm[k] += c0[k * GS] * a0;
+          Cm[k] += c1[k * GS] * a1;
+          Cm[k] += c2[k * GS] * a2;
+          Cm[k] += c3[k * GS] * a3;
+        }
+      }
+      for (; e < e1; ++e) {
         const double a = m.fo_alpha[e];
         const double *cp = sC + m.fo_spc_eff[e] * TS + q;
 #pragma unroll
@@ -179,7 +226,20 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
       kr[k] *= Pc;
     }
   }
-  if (0.0 < lim && lim < 1.0e300) {
+  if (lim_step) {  // one limit per step (perf_net.cpp:213-224)
+    const double lf = lim_step[R.fwd];
+    if (0.0 < lf && lf < 1.0e300) {
+#pragma unroll
+      for (int k = 0; k < V; ++k) kf[k] *= lf / (lf + kf[k]);
+    }
+    if (R.rev >= 0) {
+      const double lr = lim_step[R.rev];
+      if (0.0 < lr && lr < 1.0e300) {
+#pragma unroll
+        for (int k = 0; k < V; ++k) kr[k] *= lr / (lr + kr[k]);
+      }
+    }
+  } else if (0.0 < lim && lim < 1.0e300) {  // the plugin's step_limiter option
 #pragma unroll
     for (int k = 0; k < V; ++k) {
       kf[k] *= lim / (lim + kf[k]);
