@@ -49,6 +49,13 @@ def args_():
                    help="reactors of the 160-species integration workload (0: skip)")
     p.add_argument("--no-learned", action="store_true",
                    help="skip the learned-predictor form of the integration leg")
+    p.add_argument("--integration-suite", default="",
+                   help="comma-separated integration configs (c1,c3,c4,c5) to run instead of the "
+                        "rates headline: every form, with end-state tolerance verdicts")
+    p.add_argument("--suite-scale", type=float, default=1.0,
+                   help="fraction of each config's reactor count (bounded calibration runs)")
+    p.add_argument("--suite-pairs", type=int, default=1 << 20,
+                   help="training pairs of the learned predictor in the suite")
     p.add_argument("--integ-dt", type=float, default=2e-3,
                    help="integration interval per reactor in seconds (2 ms: the workload; "
                         "shorter only for bounded profiling captures)")
@@ -162,6 +169,82 @@ def cpu_reference(files, T, P, Y, budget_s=12.0, nthreads=None):
                       f"({kind} exp) + restated SetupJacobianSparse, {nthreads} OpenMP threads"}
 
 
+def reference_gpu_rates(files, T, P, Y, reps=5, n_max=1 << 18):
+    """The reference's own GPU rate path, mechanism_cuda::getReactionRates_CUDA_mr_dev
+    (src/zerork/mechanism_cuda.cu:150-156), compiled unmodified for sm_100a into
+    oracle/_ref/libzrk_ref_cuda.so, timed on the same (T, C) states beside this
+    repository's rates-from-concentrations kernel (zrk_rates_tc_dev, no limiter,
+    same outputs: net, create, destroy, rates of progress), in batches of n_max
+    reactors (the reference's nReactorsMax).  Both read T and C and write the
+    four outputs in the same species-major layout.  Returns None when the
+    library was not built."""
+    import ctypes as C
+    import torch
+    import zerork_b200 as zb
+    path = os.path.join(ROOT, "oracle", "_ref", "libzrk_ref_cuda.so")
+    if not os.path.exists(path):
+        return None
+    L = C.CDLL(path)
+    vp = C.c_void_p
+    L.zrkref_cuda_load.restype = vp
+    L.zrkref_cuda_load.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]
+    L.zrkref_cuda_free.argtypes = [vp]
+    L.zrkref_cuda_rates.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp]
+    n = len(T)
+    nb = min(n, n_max)
+    h = L.zrkref_cuda_load(files[0].encode(), files[1].encode(), os.devnull.encode(), nb)
+    if not h:
+        return None
+    pm = zb.Mechanism(*files)
+    S, N = pm.nsp, pm.nstep
+    mw = pm.table("mw")
+    rho = P / (8.314462618e3 * T * np.sum(Y / mw, axis=1))
+    conc = rho[:, None] * Y / mw
+    dev = torch.device("cuda")
+    kw = dict(dtype=torch.float64, device=dev)
+    batches = []
+    for b0 in range(0, n - nb + 1, nb):
+        Tb = torch.from_numpy(np.ascontiguousarray(T[b0:b0 + nb])).to(dev)
+        Cb = torch.from_numpy(np.ascontiguousarray(conc[b0:b0 + nb].T)).to(dev)
+        batches.append((Tb, Cb))
+    outs = [torch.empty((S, nb), **kw) for _ in range(3)] + [torch.empty((N, nb), **kw)]
+    mine = [torch.empty((S, nb), **kw) for _ in range(3)] + [torch.empty((N, nb), **kw)]
+    ptrs = [o.data_ptr() for o in outs]
+
+    def ref_step():
+        for Tb, Cb in batches:
+            L.zrkref_cuda_rates(h, nb, Tb.data_ptr(), Cb.data_ptr(), *ptrs)
+
+    def my_step():
+        for Tb, Cb in batches:
+            zb.check(zb.lib().zrk_rates_tc_dev(pm.handle, nb, nb, zb._ptr(Tb), zb._ptr(Cb), None,
+                                               *[zb._ptr(o) for o in mine], None))
+
+    res = {}
+    for name, fn in (("reference", ref_step), ("b200", my_step)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {"ms_per_step": ms, "states_per_s": len(batches) * nb / (ms / 1e3)}
+    # the two agree (last batch): net rates at 1e-12 of create + destroy
+    net_r, cre_r, des_r = (o.cpu().numpy() for o in outs[:3])
+    net_m = mine[0].cpu().numpy()
+    scale = np.abs(cre_r) + np.abs(des_r)
+    L.zrkref_cuda_free(h)
+    return {"workload": f"rates from (T, C), no Jacobian: {S} species / {N} steps, "
+                        f"{len(batches) * nb} states in batches of {nb} (nReactorsMax)",
+            "reference": res["reference"], "b200": res["b200"],
+            "ratio": res["reference"]["ms_per_step"] / res["b200"]["ms_per_step"],
+            "max_scaled_net_diff": float(np.max(np.abs(net_r - net_m) / np.maximum(scale, 1e-300))),
+            "source": "oracle/_ref/libzrk_ref_cuda.so (reference src/zerork CUDA sources, sm_100a)"}
+
+
 def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
     """Reactors integrated/s on the 160-species / 900-reaction mechanism (2 ms
     per reactor at rtol 1e-8, atol 1e-20) through the cfd_plugin API with host
@@ -252,6 +335,111 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
     return out
 
 
+INTEG_CONFIGS = {
+    # name: (mechanism spec, state workload, reactors, interval s, CPU oracle sample)
+    "c1": ("c1_h2", "c1", 64, 1e-3, 64),
+    "c3": ("c3_160", "c3", 16384, 2e-3, 32),
+    "c4": ("c4_650", "c4", 4096, 5e-3, 8),
+    "c5": ("c3_160", "c5", 16384, 2e-3, 32),
+}
+
+
+def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None):
+    """Every integration config through the cfd_plugin API (host arrays, one
+    solve call per form, reactors in the given order): plain FP64, the FP32
+    preconditioned form, the learned predictor, and FP32 + learned together.
+    Per form: reactors/s, solver counters, failed reactors, and the end-state
+    error on a sample against the CPU oracle (rtol 1e-8) and its
+    tight-tolerance run (rtol 1e-12, no per-step failure limits): the verdict
+    passes when every sampled reactor's |T - T_tight| is within 50 x the
+    oracle's own error (floored at 10 x the sample median) + 1e-5 T, and its
+    max |Y - Y_tight| within 50 x (same floor) + 1e-8, the bound of the test
+    suite (tests/test_integrator_gpu.py).  C5 trains the predictor network on
+    about `pairs` (state, interval, next state) pairs that the integrator
+    generates from other seeded states of the same mechanism."""
+    from zerork_b200 import mechgen
+    from zerork_b200.plugin import Plugin
+    import zerork_b200 as zb
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import zrk_oracle as zo
+    out = {}
+    nth = threads or os.cpu_count() or 1
+    for name in names:
+        spec, wl, nr, dt, msamp = INTEG_CONFIGS[name]
+        nr = max(8, int(nr * scale))
+        g = mechgen.generate(mechgen.SPECS[spec])
+        res = {"workload": f"{spec}: {len(g.species)} species, {nr} reactors ({wl} states), "
+                           f"{dt * 1e3:g} ms each, rtol 1e-8, atol 1e-20"}
+        with tempfile.TemporaryDirectory() as d:
+            mf, tf = g.write(d)
+            T, P, Y = mechgen.reactor_states(g, nr, "c3" if wl == "c5" else wl, seed=11)
+            net = xs = ts = None
+            forms = [("plain_fp64", 0, False), ("fp32", 1, False)]
+            if name in ("c1", "c3", "c5"):
+                from zerork_b200 import predictor as pr
+                t0 = time.perf_counter()
+                ng = max(64, min(4096, pairs // 64))
+                T0, P0, Y0 = mechgen.reactor_states(g, ng, "c3" if wl == "c5" else wl, seed=1001)
+                rounds = max(1, pairs // ng)
+                Xp, Tp = pr.generate_pairs(mf, tf, T0, P0, Y0, rounds=rounds, seed=5)
+                t_gen = time.perf_counter() - t0
+                t0 = time.perf_counter()
+                net, xs, ts, hist = pr.train(Xp, Tp, epochs=8 if Xp.shape[0] > 300000 else 12,
+                                             batch=4096, lr=1e-3)
+                res["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen,
+                                            "train_s": time.perf_counter() - t0,
+                                            "loss_first_last": [hist[0], hist[-1]]}
+                forms += [("fp64_learned", 0, True), ("fp32_learned", 1, True)]
+            ends = {}
+            for form, fp32, use_net in forms:
+                p = Plugin(mf, tf, lu_fp32=fp32)
+                if use_net:
+                    p.set_predictor(net, xs, ts)
+                Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+                t0 = time.perf_counter()
+                rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
+                wall = time.perf_counter() - t0
+                st = p.last_stats()
+                ends[form] = (Tg, Yg)
+                res[form] = {"value": nr / wall, "unit": "reactors/s", "wall_s": wall,
+                             "kernel_ms": st["kernel_ms"], "status": rc, "failed": st["nfailed"],
+                             "steps": st["nsteps"], "newton_per_step": st["nnewt"] / max(1, st["nsteps"]),
+                             "rejected": st["nrej"], "factorizations": st["nlu"],
+                             "jacobians": st["njac"],
+                             "krylov_per_newton": st["nkry"] / max(1, st["nnewt"])}
+                p.close()
+            base = res["plain_fp64"]["value"]
+            for form, _, _ in forms[1:]:
+                res[form]["over_plain"] = res[form]["value"] / base
+            # end-state error on a sample against the oracle and its tight run
+            pm = zb.Mechanism(mf, tf, device=False)
+            ot = _oracle_tables(pm, zo)
+            m = min(nr, msamp)
+            t0 = time.perf_counter()
+            To, Po, Yo, so = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth)
+            t_oracle = time.perf_counter() - t0
+            Tt, Pt, Yt, stt = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth, rtol=1e-12,
+                                       atol=1e-24, max_steps=400000, fail_caps=0)
+            ok = (so["status"] == 0) & (stt["status"] == 0)
+            res["cpu_oracle"] = {"value": m / t_oracle, "unit": "reactors/s", "cores": nth,
+                                 "kind": "port", "sample": f"first {m} reactors", "failed": int((~ok).sum())}
+            eo_T = np.abs(To - Tt)[ok]
+            eo_Y = np.max(np.abs(Yo - Yt), axis=1)[ok]
+            fT = 10 * np.median(eo_T) if eo_T.size else 0.0
+            fY = 10 * np.median(eo_Y) if eo_Y.size else 0.0
+            for form, (Tg, Yg) in ends.items():
+                eg_T = np.abs(Tg[:m] - Tt)[ok]
+                eg_Y = np.max(np.abs(Yg[:m] - Yt), axis=1)[ok]
+                bound_T = 50 * np.maximum(eo_T, fT) + 1e-5 * Tt[ok]
+                bound_Y = 50 * np.maximum(eo_Y, fY) + 1e-8
+                res[form]["max_abs_dT_vs_tight"] = float(eg_T.max()) if eg_T.size else None
+                res[form]["max_abs_dY_vs_tight"] = float(eg_Y.max()) if eg_Y.size else None
+                res[form]["oracle_max_abs_dT_vs_tight"] = float(eo_T.max()) if eo_T.size else None
+                res[form]["within_tolerance"] = bool(np.all(eg_T <= bound_T) and np.all(eg_Y <= bound_Y))
+        out[name] = res
+    return out
+
+
 def _oracle_tables(pm, zo):
     """CPU oracle tables from the product loader's tables (the loader is pinned
     bit-exact to the reference's own tables by the test suite)."""
@@ -307,6 +495,11 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", 0))
     if a.impl == "reference":
         run_reference_arm(a, rank, world)
+        return
+    if a.integration_suite:
+        res = integration_suite([x for x in a.integration_suite.split(",") if x], a.suite_scale,
+                                a.suite_pairs)
+        print(json.dumps({"integration_suite": res}))
         return
     import torch
     import torch.distributed as dist

@@ -70,7 +70,7 @@ int zrk_mech_set_double_option(zrk_mech_t m, const char *name, double value);
 int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value);
 
 /* Tile mapping of the rate kernel: ts states per tile (8/16/32), v states
- * per thread (1/2/4), warps per CTA (1..16), global_ws = 1 puts the per-tile
+ * per thread (1/2/4), warps per CTA (1..16; 32 with v = 1), global_ws = 1 puts the per-tile
  * workspace in global scratch (grid CTAs; 0 = one CTA per tile).  ts = 0
  * restores the default mapping. */
 int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int global_ws, int grid);
@@ -112,7 +112,9 @@ int zrk_rates_jac_dev(zrk_mech_t m, int n, int ld, const double *T, const double
  * ZRK_ERR_INVALID_ARGUMENT, with the sizes in zrk_last_error(), when one
  * tile's workspace alone is larger than the array.  The first call on a
  * device looks the array's device address up (cudaGetSymbolAddress) and
- * caches it: make that first call before capturing any stream.  The kernel
+ * caches it for the life of the process: make that first call before
+ * capturing any stream, and do not call this entry point on a device after
+ * a cudaDeviceReset of it (the cached address would be stale).  The kernel
  * writes every workspace word before reading it, so the array needs no
  * clearing, but all calls in the process share it: calls that overlap on
  * the GPU (different streams or handles without ordering between them)
@@ -162,6 +164,11 @@ int zrk_plugin_last_stats(struct zerork_handle_impl *h, long *totals7, float *ke
  * preconditioned FP64 GMRES; 0 on the FP64 path).  No counterpart in the
  * reference beyond CVODE's linear-iteration counter. */
 int zrk_plugin_krylov_iterations(struct zerork_handle_impl *h, long *iterations);
+
+/* Species count of the handle's loaded mechanism (the step callback's y and
+ * dy hold nsp + 1 entries: mass fractions, then T / Tref), or -1 before
+ * zerork_reactor_load_mechanism.  No counterpart in the reference. */
+int zrk_plugin_num_species(struct zerork_handle_impl *h);
 
 /* Every zerork_reactor_solve call runs as one CUDA graph (copies in, work
  * queue reset, the persistent integration kernel, copies out), captured when

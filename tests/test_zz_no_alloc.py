@@ -64,10 +64,18 @@ def test_no_alloc_matches_rates_jac_dev_on_consecutive_calls(torch, mech_dir):
     L.zrk_last_error.restype = C.c_char_p
     g, (mf, tf) = synth("c2_53", mech_dir)
     pm = zb.Mechanism(mf, tf)
+    # an explicit tile mapping, so the workspace slice size is known: rows of
+    # ts doubles (C, u/RT, g/RT, one per step, two partial buffers per warp,
+    # two more), ZRK_NOALLOC_SCRATCH_BYTES = 8 MiB of them
+    ts, v, warps = 16, 2, 8
+    pm.set_launch(ts, v, warps, False, 0)
+    slice_bytes = (3 * pm.nsp + pm.nstep + 2 * warps + 2) * ts * 8
+    slices = (8 << 20) // slice_bytes
     ot = oracle_tables(zb.Mechanism(mf, tf, device=False))
     # two calls in a row with different sizes and states: the second must not
     # see anything the first left in the shared workspace; 3000 states give
     # more tiles than the fixed array holds slices for, so CTAs take several
+    assert -(-3000 // ts) > slices
     for n, ld, seed in ((3000, 3008, 1), (517, 517, 2)):
         T, P, Y = mechgen.rate_states(g, n, seed=seed)
         inputs = _device_inputs(torch, pm, T, P, Y, ld)

@@ -260,7 +260,7 @@ int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   for (int ts : {8, 16, 32})
     for (int v : {1, 2, 4})
-      for (int warps : {4, 8, 16}) {
+      for (int warps : {4, 8, 16, 32}) {
         LaunchCfg c;
         c.ts = ts;
         c.v = v;
@@ -402,8 +402,11 @@ int zrk_rates_jac_host(zrk_mech_t m, int n, const double *T, const double *P, co
   MechHandle *h = reinterpret_cast<MechHandle *>(m);
   if (!h->dev) return set_error(ZRK_ERR_NO_DEVICE, "handle has no device tables (zrk_mech_parse)");
   const int S = h->tables.nsp, nnz = h->pattern.nnz;
-  // Two-slot pipeline: chunk i uses stream/slot i%2, so the copies of one
-  // chunk overlap the kernel of the other.  Device slots are cached.
+  // Two-slot pipeline: chunk i uses stream/slot i%2, so with pinned host
+  // buffers the copies of one chunk overlap the kernel of the other
+  // (pageable buffers are staged by the driver and overlap little; the
+  // global-workspace mapping shares one scratch area and uses one stream).
+  // Device slots are cached.
   const size_t per_state = sizeof(double) * (2 + 2 * (size_t)S + (jac ? nnz : 0));
   long chunk = (long)((512ull << 20) / per_state);
   chunk = std::max(1024L, std::min<long>(chunk, n));

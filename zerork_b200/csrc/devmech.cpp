@@ -197,6 +197,9 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   size_t o_jw = b.add(jw), o_jt = b.add(jt), o_jtp = b.add(jt_ptr), o_jc = b.add(jcost),
          o_jf = b.add(jf_ptr);
   size_t o_ro = b.add(rxn_order), o_so = b.add(spc_order), o_co = b.add(col_order);
+  std::vector<RxnRec> rec_by_cost;
+  for (int p : rxn_order) rec_by_cost.push_back(rec[p]);
+  size_t o_rbc = b.add(rec_by_cost);
   bytes_ = b.bytes.size();
   check(cudaMalloc(&blob_, bytes_), "cudaMalloc(mechanism tables)");
   check(cudaMemcpy(blob_, b.bytes.data(), bytes_, cudaMemcpyHostToDevice), "cudaMemcpy(mechanism tables)");
@@ -250,6 +253,7 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   view_.rxn_order = (const int *)P(o_ro);
   view_.spc_order = (const int *)P(o_so);
   view_.col_order = (const int *)P(o_co);
+  view_.rxn_by_cost = (const RxnRec *)P(o_rbc);
 }
 
 DeviceMechanism::~DeviceMechanism() {

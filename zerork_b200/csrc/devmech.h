@@ -76,6 +76,9 @@ struct DevMech {
   // assignment to thread groups: reactions, species (production gathers),
   // species Jacobian columns
   const int *rxn_order, *spc_order, *col_order;
+  // the reaction records in rxn_order order (position p holds reaction
+  // rxn_order[p]): one load instead of two dependent ones per work item
+  const RxnRec *rxn_by_cost;
 };
 
 // Host-side builder; owns the device allocation.

@@ -458,7 +458,7 @@ template <class LT>
 __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o, const BdfConst &bc,
                            const Warp &w, const Vecs &V, LT *LU, double v, double t_end,
                            double rtol, double atol, ReactorStats &st, int lane, double &t_done,
-                           double t_off, double T_target, double &t_ign) {
+                           double t_off, double T_target, double &t_ign, CbCtx &cb) {
   const int n = m.nsp + 1;
   LT *x = (LT *)w.X;
   double t = 0.0;
@@ -670,14 +670,23 @@ __device__ int bdf_attempt(const DevMech &m, const LUDev &lu, const IntegOpts &o
       if (t_ign < 0.0 && Tn >= T_target) {
         const double frac = (Tn > T_prev) ? (T_target - T_prev) / (Tn - T_prev) : 1.0;
         t_ign = t_off + (t - h) + frac * h;
-        if (o.stop_ign) {  // stop_after_ignition: the call ends at the crossing
-          for (int i = lane; i < n; i += 32) V.y[i] = V.tmp[i] + frac * (V.D[i] - V.tmp[i]);
+        // the callback's record of CVode's root return (solver_cvode.cpp:249-262)
+        const bool cb_end = cb.rec && cb_record(cb, V.D, o.stop_ign ? V.tmp : nullptr, n, q, h,
+                                                frac - 1.0, frac, t_ign, V.y, lane, 32);
+        if (o.stop_ign || cb_end) {  // stop_after_ignition: the call ends at the crossing
+          if (!cb_end)
+            for (int i = lane; i < n; i += 32) V.y[i] = V.tmp[i] + frac * (V.D[i] - V.tmp[i]);
           __syncwarp();
           t_done = (t - h) + frac * h;
           return 0;
         }
       }
       T_prev = Tn;
+    }
+    if (cb.rec && cb_record(cb, V.D, nullptr, n, q, h, 0.0, 0.0, t_off + t, V.y, lane, 32)) {
+      __syncwarp();  // the callback asked to stop here
+      t_done = t;
+      return 0;
     }
     if (neq < q + 1) continue;
     double em = INFINITY, ep = INFINITY;
@@ -793,6 +802,8 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     if (lane == 0) V.y[S] = T0 / o.Tref;
     __syncwarp();
     ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    CbCtx cb{a.cb_rec ? a.cb_rec + (size_t)idx * a.cb_cap * (3 + 2 * (size_t)n) : nullptr, a.cb_cap,
+             (a.cb_rec && a.cb_stop) ? a.cb_stop[r] : 0, 0, 0, 0.0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
     double t_left = a.dt, t_ign = -1.0;
@@ -801,8 +812,9 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     for (int attempt = 0;; ++attempt) {
       double t_done = 0.0;
       rc = bdf_attempt<LT>(m, lu, o, bc, w, V, LU, v, t_left, rtol, atol, rs, lane, t_done, a.dt - t_left,
-                           T_target, t_ign);
+                           T_target, t_ign, cb);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
+      cb.ncalls++;  // the failed CVode call counts as a step
       t_left -= t_done;
       // solver_cvode.cpp:236-246: adjust tolerances and start over from the
       // last accepted state for the remaining time
@@ -830,6 +842,7 @@ __global__ void __launch_bounds__(384, 1) integrate_kernel(DevMech m, LUDev lu, 
     if (lane == 0) {
       a.v[r] = v;
       if (a.stats) a.stats[r] = rs;
+      if (a.cb_cnt) a.cb_cnt[r] = cb.cnt;
       if (a.t_ign) a.t_ign[r] = t_ign;
     }
     __syncwarp();

@@ -77,6 +77,65 @@ struct ReactorStats {
   int pad;
 };
 
+// Per-step records for the plugin's step callback
+// (zerork_reactor_set_callback_fn; solver_cvode.cpp:247-257 calls it after
+// every successful CVode call with the state and the interpolant's
+// derivative).  With rec set, each accepted step of the reactor appends one
+// record of 3 + 2n doubles {t from the call's start, t - previous record's t,
+// the reference's call counter, y[n], dy/dt[n]}, up to cap records; cnt
+// counts every record, also past the cap.  The first crossing of the
+// ignition temperature adds a record at the crossing before the step's own,
+// as CVode's root return does.  stop > 0 ends the reactor's call at its
+// stop-th record, with that record's state.
+struct CbCtx {
+  double *rec;
+  int cap, stop;
+  int cnt, ncalls;
+  double tprev;
+};
+
+#ifdef __CUDACC__
+// Appends one callback record at x = (t_rec - t) / h in [-1, 0] of the step
+// just accepted (x = 0: the step itself): y and y' of the backward-difference
+// interpolant sum_k D_k prod_{j<k} (x + j) / (j + 1) through the last q + 1
+// steps, or, with prev set, y = prev + wprev (D_0 - prev) (the state
+// stop_after_ignition gives the crossing).  Threads i0, i0 + di, ... share the
+// entries.  Returns true when this record ends the call; then ystop (all n
+// entries) holds the record's y.
+__device__ inline bool cb_record(CbCtx &cb, const double *D, const double *prev, int n, int q,
+                                 double h, double x, double wprev, double tabs, double *ystop,
+                                 int i0, int di) {
+  cb.ncalls++;
+  const bool stop = cb.stop > 0 && cb.cnt + 1 >= cb.stop;
+  double *e = cb.cnt < cb.cap ? cb.rec + (size_t)cb.cnt * (3 + 2 * n) : nullptr;
+  if (e && i0 == 0) {
+    e[0] = tabs;
+    e[1] = tabs - cb.tprev;
+    e[2] = (double)cb.ncalls;
+  }
+  if (e || stop) {
+    for (int i = i0; i < n; i += di) {
+      double c = 1.0, dc = 0.0, y = D[i], yd = 0.0;
+      for (int k = 1; k <= q; ++k) {
+        dc = (dc * (x + k - 1) + c) / k;
+        c = c * (x + k - 1) / k;
+        y += D[k * n + i] * c;
+        yd += D[k * n + i] * dc;
+      }
+      if (prev) y = prev[i] + wprev * (D[i] - prev[i]);
+      if (e) {
+        e[3 + i] = y;
+        e[3 + n + i] = yd / h;
+      }
+      if (stop) ystop[i] = y;
+    }
+  }
+  cb.cnt++;
+  cb.tprev = tabs;
+  return stop;
+}
+#endif
+
 struct IntegArgs {
   int n_reactors;
   const int *order;         // queue order (reactor indices), may be null
@@ -95,6 +154,14 @@ struct IntegArgs {
   const double *dpdt;       // optional pressure rates [n_reactors] (Pa/s)
   const double *esrc;       // optional energy sources [n_reactors] (J/kg/s)
   const double *tdel_in;    // previous temperature deltas [n_reactors] (read when !always_T)
+  // step-callback records (CbCtx): cb_cap records of 3 + 2 (nsp + 1) doubles
+  // per work-queue position (the reactor order[i] writes slot i), cb_cnt
+  // [reactor] step counts, cb_stop [reactor] (may be null) steps after which
+  // a reactor's call ends (0: none); all null when no callback is set
+  double *cb_rec;
+  int cb_cap;
+  int *cb_cnt;
+  const int *cb_stop;
 };
 
 size_t integ_smem_per_warp(const DevMech &m, const LUDev &lu, bool rop_in_smem);

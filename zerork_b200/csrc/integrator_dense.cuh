@@ -131,7 +131,7 @@ __device__ __noinline__ int rhs_cta(const DevMech &m, const IntegOpts &o, const 
   for (int rr = 0; rr * nt < m.nrxn; ++rr) {
     const int pos = rr * nt + ((rr & 1) ? nt - 1 - tid : tid);
     if (pos < m.nrxn)
-      reaction_item<1, 1>(m, load_rxn(m.rxn + m.rxn_order[pos]), 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum,
+      reaction_item<1, 1>(m, load_rxn(m.rxn_by_cost + pos), 0, s.C, s.G, s.ROP, &T, &logT, &invT, &lprt, &Csum,
                           o.lim);
   }
   __syncthreads();
@@ -756,7 +756,7 @@ template <class LT>
 __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o, const Consts &bc, const Smem &s,
                            double *J, double v, double t_end, double rtol, double atol,
                            ReactorStats &st, int lda, double &t_done, double t_off, double T_target,
-                           double &t_ign) {
+                           double &t_ign, CbCtx &cb) {
   const int n = m.nsp + 1, tid = threadIdx.x, nt = blockDim.x;
   const int nc = (n + 31) / 32;
   auto vrms = [&](const double *x, const double *sc) {
@@ -993,14 +993,23 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
       if (t_ign < 0.0 && Tn >= T_target) {
         const double frac = (Tn > T_prev) ? (T_target - T_prev) / (Tn - T_prev) : 1.0;
         t_ign = t_off + (t - h) + frac * h;
-        if (o.stop_ign) {  // stop_after_ignition: the call ends at the crossing
-          for (int i = tid; i < n; i += nt) s.y[i] = s.tmp[i] + frac * (s.D[i] - s.tmp[i]);
+        // the callback's record of CVode's root return (solver_cvode.cpp:249-262)
+        const bool cb_end = cb.rec && cb_record(cb, s.D, o.stop_ign ? s.tmp : nullptr, n, q, h,
+                                                frac - 1.0, frac, t_ign, s.y, tid, nt);
+        if (o.stop_ign || cb_end) {  // stop_after_ignition: the call ends at the crossing
+          if (!cb_end)
+            for (int i = tid; i < n; i += nt) s.y[i] = s.tmp[i] + frac * (s.D[i] - s.tmp[i]);
           __syncthreads();
           t_done = (t - h) + frac * h;
           return 0;
         }
       }
       T_prev = Tn;
+    }
+    if (cb.rec && cb_record(cb, s.D, nullptr, n, q, h, 0.0, 0.0, t_off + t, s.y, tid, nt)) {
+      __syncthreads();  // the callback asked to stop here
+      t_done = t;
+      return 0;
     }
     if (neq < q + 1) continue;
     double em = INFINITY, ep = INFINITY;
@@ -1121,6 +1130,8 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     if (tid == 0) s.y[S] = T0 / o.Tref;
     __syncthreads();
     ReactorStats rs = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    CbCtx cb{a.cb_rec ? a.cb_rec + (size_t)idx * a.cb_cap * (3 + 2 * (size_t)n) : nullptr, a.cb_cap,
+             (a.cb_rec && a.cb_stop) ? a.cb_stop[r] : 0, 0, 0, 0.0};
     double rtol = o.rtol, atol = o.atol;
     int rc = 0;
     // retries (solver_cvode.cpp:227-246): restart the method from the last
@@ -1132,8 +1143,9 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     for (int attempt = 0;; ++attempt) {
       double t_done = 0.0;
       rc = attempt_cta<LT>(m, o, bc, s, J, v, t_left, rtol, atol, rs, lda, t_done, a.dt - t_left,
-                               T_target, t_ign);
+                               T_target, t_ign, cb);
       if (rc == 0 || attempt + 1 >= o.max_retries) break;
+      cb.ncalls++;  // the failed CVode call counts as a step
       t_left -= t_done;
       rs.retries++;
       atol *= o.retry_atol_factor;
@@ -1158,6 +1170,7 @@ __global__ void __launch_bounds__(512, 1) integrate_dense_kernel(DevMech m, Inte
     if (tid == 0) {
       a.v[r] = v;
       if (a.stats) a.stats[r] = rs;
+      if (a.cb_cnt) a.cb_cnt[r] = cb.cnt;
       if (a.t_ign) a.t_ign[r] = t_ign;
     }
     __syncthreads();

@@ -105,6 +105,15 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
   for (int snake_r = 0, var = 0; snake_r * NG < (count); ++snake_r)  \
     if (const int snake_p = snake_r * NG + ((snake_r & 1) ? NG - 1 - g : g); \
         snake_p < (count) && ((var = (list)[snake_p]), true))
+// All reactions: the cost-sorted records (devmech.h rxn_by_cost) in snake
+// order over the groups.
+#define RXN_PASS(CONC, CSUM)                                                          \
+  for (int rr_ = 0; rr_ * NG < m.nrxn; ++rr_) {                                      \
+    const int rp_ = rr_ * NG + ((rr_ & 1) ? NG - 1 - g : g);                         \
+    if (rp_ < m.nrxn)                                                                \
+      reaction_item<TS, V>(m, load_rxn(m.rxn_by_cost + rp_), q, CONC, sG, sROP, Tr, logT, invT, \
+                           lprt, CSUM, kp.lim);                                      \
+  }
   const int ntiles = (n + TS - 1) / TS;
   const double dummy_y = 1.0 / S;
 
@@ -193,8 +202,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       cvc[k] = c2;
     }
     // ---- reactions at T
-    SNAKE(r, m.rxn_order, m.nrxn)
-      reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
+    RXN_PASS(sC, Csum)
     __syncthreads();
     // ---- net production rates, energy partial
     {
@@ -271,8 +279,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           Cc[k] = cs;
           cvc[k] = c2;
         }
-        SNAKE(r, m.rxn_order, m.nrxn)
-          reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, Tr, logT, invT, lprt, Cc, kp.lim);
+        RXN_PASS(sC, Cc)
       }
       __syncthreads();  // also fences the reads of PT(0), PT(1) above
       {
@@ -451,8 +458,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       for (int ww = 0; ww < NW; ++ww) c2 += PT(1, ww, k);
       cvp[k] = c2;
     }
-    SNAKE(r, m.rxn_order, m.nrxn)
-      reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, Tr, logT, invT, lprt, Csum, kp.lim);
+    RXN_PASS(sC, Csum)
     __syncthreads();
     {
       double pe[V];
@@ -501,6 +507,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
 #undef PT
 #undef FORV
 #undef SNAKE
+#undef RXN_PASS
 }
 
 template <int TS, int V, int MAXT>
@@ -534,13 +541,16 @@ cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams 
   return cudaGetLastError();
 }
 
-// Up to 8 warps per CTA the kernel may use 255 registers per thread; with
-// more warps it is compiled for at most 128.
+// Up to 8 warps per CTA the kernel may use 255 registers per thread, up to
+// 16 warps 128, and with 32 warps (one state per thread only) 64: twice the
+// resident warps to hide latency with.
 template <int TS, int V>
 cudaError_t launch_tv(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
                       const LaunchCfg &cfg, cudaStream_t stream) {
   if (cfg.warps <= 8) return launch_tvm<TS, V, 256>(m, a, kp, cfg, stream);
-  return launch_tvm<TS, V, 512>(m, a, kp, cfg, stream);
+  if (cfg.warps <= 16) return launch_tvm<TS, V, 512>(m, a, kp, cfg, stream);
+  if constexpr (V == 1) return launch_tvm<TS, V, 1024>(m, a, kp, cfg, stream);
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace
@@ -551,7 +561,8 @@ size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg) {
 }
 
 bool rates_jac_mapping_ok(const LaunchCfg &c) {
-  if (c.warps < 1 || c.warps > 16) return false;
+  if (c.warps < 1 || c.warps > 32) return false;
+  if (c.warps > 16 && c.v != 1) return false;  // 64 registers per thread: one state each
   switch (c.ts * 8 + c.v) {
     case 8 * 8 + 1: case 8 * 8 + 2: case 8 * 8 + 4:
     case 16 * 8 + 1: case 16 * 8 + 2: case 16 * 8 + 4:

@@ -212,7 +212,7 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
         lPr = lPr / (nT - 0.14 * lPr);
         lPr *= lPr;
         fT /= (1.0 + lPr);
-        fT = pow(10.0, fT);
+        fT = exp10(fT);
       } else if (ty == kSRI) {
         const double xp = 1.0 / (1.0 + lPr * lPr);
         fT = p[3] * exp(-p[4] * invT[k]);

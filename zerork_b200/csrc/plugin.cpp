@@ -257,10 +257,16 @@ zerork_status_t zerork_reactor_solve(const int n_cycle, const double time, const
   const int ns = h->solver->nsp();
   // aux sources (zerork_reactor_manager.cpp:1092-1104): DPDT, E_SRC and
   // Y_SRC per reactor where the caller set them
+  // the per-step callback and reactor ids (solver_cvode.cpp:247-257,
+  // zerork_reactor_manager.cpp:1105-1108)
+  zrk::StepCallback cbs;
+  cbs.fn = h->cb;
+  cbs.data = h->cb_data;
+  cbs.reactor_ids = h->reactor_ids;
   int nfail = h->solver->solve(o, n, dt, T, P, mf, ns, cost, gpu, tdel,
                                D["solve_temperature_threshold"], nullptr, &h->last,
                                h->aux[ZERORK_FIELD_Y_SRC], ign, h->aux[ZERORK_FIELD_DPDT],
-                               h->aux[ZERORK_FIELD_E_SRC]);
+                               h->aux[ZERORK_FIELD_E_SRC], h->cb ? &cbs : nullptr);
   if (nfail < 0) {
     h->last_error = h->solver->last_error;
     std::fprintf(stderr, "zerork_b200: %s\n", h->last_error.c_str());
@@ -354,6 +360,10 @@ int zrk_plugin_krylov_iterations(zerork_handle h, long *iterations) {
   if (!h) return ZRK_ERR_INVALID_HANDLE;
   if (iterations) *iterations = h->last.nkry;
   return ZRK_OK;
+}
+
+int zrk_plugin_num_species(zerork_handle h) {
+  return (h && h->solver) ? h->solver->nsp() : -1;
 }
 
 int zrk_plugin_graph_stats(zerork_handle h, long *captures, long *launches) {

@@ -54,6 +54,7 @@ ReactorSolver::~ReactorSolver() {
   cudaFreeHost(hsrc_); cudaFreeHost(hign_); cudaFree(dsrc_); cudaFree(dign_);
   cudaFreeHost(hde_); cudaFree(dde_);
   cudaFree(lu_blob_);
+  cudaFree(dcb_rec_); cudaFree(dcb_cnt_); cudaFree(dcb_stop_); cudaFree(dcb_order_);
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_); cudaFree(drop_);
   if (ev0_) cudaEventDestroy(ev0_);
@@ -111,11 +112,178 @@ cudaError_t ReactorSolver::reserve(int n, bool fp32) {
   return cudaSuccess;
 }
 
+// Solve with the plugin's step callback: every accepted step is recorded on
+// the device (integrator.h CbCtx) and the callback runs on the host, reactor
+// by reactor and step by step, after the integration (a host function cannot
+// run inside the kernel).  Reactors with more steps than the record capacity
+// are integrated again with room for all of their steps (the integration is
+// deterministic, so the steps are the same), and reactors whose callback
+// returned nonzero are integrated again up to that step, which ends their
+// call with that step's state, as the reference's break out of its step loop
+// does (solver_cvode.cpp:247-257).  Staging: hT_/hP_/hY_ hold the inputs on
+// entry and the results on return; hstats_ and hign_ the results.
+cudaError_t ReactorSolver::solve_with_callback(int method, const IntegOpts &io, IntegArgs a,
+                                               int dthreads, int dctas, int spill, int W, int ctas,
+                                               bool rop_smem, int n, double dt,
+                                               const StepCallback &cb) {
+  const int S = tables_.nsp, nv = S + 1;
+  const size_t rec = 3 + 2 * (size_t)nv;
+  const size_t kBudget = (size_t)1 << 30;  // record memory per launch
+  const long steps_max = (long)io.max_steps * io.max_retries;
+  cudaStream_t s = stream_;
+  cudaError_t e;
+  auto ensure = [&](size_t rec_bytes) -> cudaError_t {
+    if (dcb_n_ < n) {
+      cudaFree(dcb_cnt_);
+      cudaFree(dcb_stop_);
+      cudaFree(dcb_order_);
+      dcb_cnt_ = dcb_stop_ = dcb_order_ = nullptr;
+      dcb_n_ = 0;
+      cudaError_t r;
+      if ((r = cudaMalloc(&dcb_cnt_, n * sizeof(int))) != cudaSuccess) return r;
+      if ((r = cudaMalloc(&dcb_stop_, n * sizeof(int))) != cudaSuccess) return r;
+      if ((r = cudaMalloc(&dcb_order_, n * sizeof(int))) != cudaSuccess) return r;
+      dcb_n_ = n;
+    }
+    if (dcb_bytes_ < rec_bytes) {
+      cudaFree(dcb_rec_);
+      dcb_rec_ = nullptr;
+      dcb_bytes_ = 0;
+      cudaError_t r = cudaMalloc(&dcb_rec_, rec_bytes);
+      if (r != cudaSuccess) return r;
+      dcb_bytes_ = rec_bytes;
+    }
+    return cudaSuccess;
+  };
+  // inputs as staged by solve(), kept for the repeated integrations
+  const std::vector<double> T0(hT_, hT_ + n), P0(hP_, hP_ + n), Y0(hY_, hY_ + (size_t)n * S);
+  std::vector<double> Tr(n), Pr(n), Yr((size_t)n * S), ign(n, -1.0);
+  std::vector<ReactorStats> str(n);
+  std::vector<int> cnt(n, 0);
+  // one integration of the reactors in `sel` from their initial states, with
+  // `cap` records each and per-reactor stops (empty: none); results merged
+  auto run = [&](const std::vector<int> &sel, int cap, const std::vector<int> &stop,
+                 std::vector<double> *recs) -> cudaError_t {
+    const int m = (int)sel.size();
+    cudaError_t r;
+    if ((r = ensure((size_t)m * cap * rec * sizeof(double))) != cudaSuccess) return r;
+    std::memcpy(hT_, T0.data(), n * sizeof(double));
+    std::memcpy(hP_, P0.data(), n * sizeof(double));
+    std::memcpy(hY_, Y0.data(), (size_t)n * S * sizeof(double));
+    std::memcpy(horder_, sel.data(), m * sizeof(int));
+    if ((r = cudaMemcpyAsync(dT_, hT_, n * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (r = cudaMemcpyAsync(dP_, hP_, n * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (r = cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess ||
+        (r = cudaMemcpyAsync(dcb_order_, horder_, m * sizeof(int), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess ||
+        (a.ysrc && (r = cudaMemcpyAsync(dsrc_, hsrc_, (size_t)n * S * sizeof(double),
+                                        cudaMemcpyHostToDevice, s)) != cudaSuccess) ||
+        (a.dpdt && (r = cudaMemcpyAsync(dde_, hde_, n * sizeof(double), cudaMemcpyHostToDevice, s)) !=
+                       cudaSuccess) ||
+        (a.esrc && (r = cudaMemcpyAsync(dde_ + cap_, hde_ + cap_, n * sizeof(double),
+                                        cudaMemcpyHostToDevice, s)) != cudaSuccess) ||
+        (a.tdel_in && (r = cudaMemcpyAsync(dde_ + 2 * cap_, hde_ + 2 * cap_, n * sizeof(double),
+                                           cudaMemcpyHostToDevice, s)) != cudaSuccess) ||
+        (r = cudaMemsetAsync(dhead_, 0, sizeof(int), s)) != cudaSuccess ||
+        (r = cudaMemsetAsync(dcb_cnt_, 0, n * sizeof(int), s)) != cudaSuccess)
+      return r;
+    if (!stop.empty() &&
+        (r = cudaMemcpyAsync(dcb_stop_, stop.data(), n * sizeof(int), cudaMemcpyHostToDevice, s)) !=
+            cudaSuccess)
+      return r;
+    IntegArgs b = a;
+    b.n_reactors = m;
+    b.order = dcb_order_;
+    b.cb_rec = dcb_rec_;
+    b.cb_cap = cap;
+    b.cb_cnt = dcb_cnt_;
+    b.cb_stop = stop.empty() ? nullptr : dcb_stop_;
+    if ((r = cudaEventRecord(ev0_, s)) != cudaSuccess) return r;
+    r = method == 1 ? launch_integrate_dense(dm_->view(), io, b, dthreads, std::min(dctas, m), spill, s)
+                    : launch_integrate(dm_->view(), lud_, io, b, W, ctas, rop_smem, s);
+    if (r != cudaSuccess) return r;
+    if ((r = cudaEventRecord(ev1_, s)) != cudaSuccess) return r;
+    std::vector<int> c(n);
+    if ((r = cudaMemcpyAsync(hT_, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (r = cudaMemcpyAsync(hP_, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (r = cudaMemcpyAsync(hY_, dY_, (size_t)n * S * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (r = cudaMemcpyAsync(hstats_, dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (a.t_ign && (r = cudaMemcpyAsync(hign_, dign_, n * sizeof(double), cudaMemcpyDeviceToHost, s)) !=
+                        cudaSuccess) ||
+        (r = cudaMemcpyAsync(c.data(), dcb_cnt_, n * sizeof(int), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return r;
+    if (recs) {  // slot i holds the records of sel[i]
+      recs->resize((size_t)m * cap * rec);
+      if ((r = cudaMemcpyAsync(recs->data(), dcb_rec_, recs->size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+        return r;
+    }
+    if ((r = cudaStreamSynchronize(s)) != cudaSuccess) return r;
+    for (int k : sel) {
+      Tr[k] = hT_[k];
+      Pr[k] = hP_[k];
+      std::memcpy(&Yr[(size_t)k * S], &hY_[(size_t)k * S], S * sizeof(double));
+      str[k] = hstats_[k];
+      if (a.t_ign) ign[k] = hign_[k];
+      cnt[k] = c[k];
+    }
+    return cudaSuccess;
+  };
+  std::vector<int> all(n), slot(n);
+  for (int k = 0; k < n; ++k) all[k] = horder_[k];  // the cost order solve() chose
+  for (int i = 0; i < n; ++i) slot[all[i]] = i;
+  int cap = (int)std::max<long>(
+      8, std::min<long>(steps_max, (long)(kBudget / ((size_t)n * rec * sizeof(double)))));
+  cap = std::min(cap, 4096);
+  std::vector<double> recs;
+  if ((e = run(all, cap, {}, &recs)) != cudaSuccess) return e;
+  // callbacks in reactor order; reactors past the capacity are integrated
+  // again alone with room for all of their steps
+  std::vector<int> stop(n, 0);
+  bool any_stop = false;
+  std::vector<double> more;
+  for (int k = 0; k < n; ++k) {
+    const double *base = recs.data() + (size_t)slot[k] * cap * rec;
+    if (cnt[k] > cap) {
+      const int keep = cnt[k];
+      if ((e = run({k}, keep, {}, &more)) != cudaSuccess) return e;
+      if (cnt[k] != keep) return cudaErrorUnknown;  // a replay must take the same steps
+      base = more.data();
+    }
+    const int id = cb.reactor_ids ? cb.reactor_ids[k] : k;
+    for (int i = 0; i < cnt[k]; ++i) {
+      const double *r0 = base + (size_t)i * rec;
+      if (cb.fn(id, (int)r0[2], r0[0], r0[1], r0 + 3, r0 + 3 + nv, cb.data) != 0) {
+        if (i + 1 < cnt[k]) {
+          stop[k] = i + 1;
+          any_stop = true;
+        }
+        break;
+      }
+    }
+  }
+  if (any_stop) {  // the reactors whose callback ended their call early
+    std::vector<int> sel;
+    for (int k = 0; k < n; ++k)
+      if (stop[k] > 0) sel.push_back(k);
+    if ((e = run(sel, 1, stop, nullptr)) != cudaSuccess) return e;
+  }
+  std::memcpy(hT_, Tr.data(), n * sizeof(double));
+  std::memcpy(hP_, Pr.data(), n * sizeof(double));
+  std::memcpy(hY_, Yr.data(), (size_t)n * S * sizeof(double));
+  std::memcpy(hstats_, str.data(), n * sizeof(ReactorStats));
+  if (a.t_ign) std::memcpy(hign_, ign.data(), n * sizeof(double));
+  return cudaSuccess;
+}
+
 int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, double *P, double *mf,
                          int stride, double *cost, double *gpu_time, double *temp_delta,
                          double temp_threshold, std::vector<ReactorStats> *stats,
                          SolveStatsTotals *tot, const double *ysrc, double *t_ign,
-                         const double *dpdt, const double *esrc) {
+                         const double *dpdt, const double *esrc, const StepCallback *cb) {
   if (n <= 0) return 0;
   const int S = tables_.nsp;
   cudaError_t e = reserve(n, o.lu_fp32);
@@ -250,73 +418,82 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     a.state = dstate_;
     a.state_stride = m.nnz;
   }
-  // The whole call (copies in, queue reset, the persistent kernel between
-  // two timing events, copies out) is one CUDA graph, captured once per
-  // configuration and replayed while nothing it depends on changes.
-  std::vector<unsigned char> key;
-  auto put_key = [&](const void *p, size_t b) {
-    key.insert(key.end(), (const unsigned char *)p, (const unsigned char *)p + b);
-  };
-  const int kv[9] = {n, method, dthreads, dctas, spill, W, ctas, rop_smem ? 1 : 0, S};
-  put_key(kv, sizeof(kv));
-  put_key(&io, sizeof(io));
-  put_key(&a, sizeof(a));
-  if (!graph_ || key != graph_key_) {
-    if (graph_) cudaGraphExecDestroy(graph_);
-    graph_ = nullptr;
-    graph_key_.clear();
-    if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
-      last_error = std::string("graph capture: ") + cudaGetErrorString(e);
+  const bool with_cb = cb && cb->fn;
+  if (with_cb) {
+    if ((e = solve_with_callback(method, io, a, dthreads, dctas, spill, W, ctas, rop_smem, n, dt, *cb)) !=
+        cudaSuccess) {
+      last_error = std::string("integration with step callback: ") + cudaGetErrorString(e);
       return -1;
     }
-    cudaError_t ce = cudaSuccess;
-    auto q = [&](cudaError_t r) {
-      if (ce == cudaSuccess) ce = r;
+  } else {
+    // The whole call (copies in, queue reset, the persistent kernel between
+    // two timing events, copies out) is one CUDA graph, captured once per
+    // configuration and replayed while nothing it depends on changes.
+    std::vector<unsigned char> key;
+    auto put_key = [&](const void *p, size_t b) {
+      key.insert(key.end(), (const unsigned char *)p, (const unsigned char *)p + b);
     };
-    q(cudaMemcpyAsync(dT_, hT_, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    q(cudaMemcpyAsync(dP_, hP_, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    q(cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
-    q(cudaMemcpyAsync(dorder_, horder_, n * sizeof(int), cudaMemcpyHostToDevice, s));
-    if (a.ysrc) q(cudaMemcpyAsync(dsrc_, hsrc_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (a.dpdt) q(cudaMemcpyAsync(dde_, hde_, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (a.esrc)
-      q(cudaMemcpyAsync(dde_ + cap_, hde_ + cap_, n * sizeof(double), cudaMemcpyHostToDevice, s));
-    if (a.tdel_in)
-      q(cudaMemcpyAsync(dde_ + 2 * cap_, hde_ + 2 * cap_, n * sizeof(double),
-                        cudaMemcpyHostToDevice, s));
-    q(cudaMemsetAsync(dhead_, 0, sizeof(int), s));
-    q(cudaEventRecordWithFlags(ev0_, s, cudaEventRecordExternal));  // a timing node in the graph
-    q(method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)
-                  : launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s));
-    q(cudaEventRecordWithFlags(ev1_, s, cudaEventRecordExternal));
-    q(cudaMemcpyAsync(hT_, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    q(cudaMemcpyAsync(hP_, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    q(cudaMemcpyAsync(hY_, dY_, (size_t)n * S * sizeof(double), cudaMemcpyDeviceToHost, s));
-    q(cudaMemcpyAsync(hstats_, dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s));
-    if (a.t_ign) q(cudaMemcpyAsync(hign_, dign_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
-    cudaGraph_t g = nullptr;
-    const cudaError_t ee = cudaStreamEndCapture(s, &g);
-    if (ce == cudaSuccess) ce = ee;
-    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&graph_, g, 0);
-    if (g) cudaGraphDestroy(g);
-    if (ce != cudaSuccess) {
+    const int kv[9] = {n, method, dthreads, dctas, spill, W, ctas, rop_smem ? 1 : 0, S};
+    put_key(kv, sizeof(kv));
+    put_key(&io, sizeof(io));
+    put_key(&a, sizeof(a));
+    if (!graph_ || key != graph_key_) {
+      if (graph_) cudaGraphExecDestroy(graph_);
       graph_ = nullptr;
-      last_error = std::string("graph capture: ") + cudaGetErrorString(ce);
+      graph_key_.clear();
+      if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed)) != cudaSuccess) {
+        last_error = std::string("graph capture: ") + cudaGetErrorString(e);
+        return -1;
+      }
+      cudaError_t ce = cudaSuccess;
+      auto q = [&](cudaError_t r) {
+        if (ce == cudaSuccess) ce = r;
+      };
+      q(cudaMemcpyAsync(dT_, hT_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+      q(cudaMemcpyAsync(dP_, hP_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+      q(cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
+      q(cudaMemcpyAsync(dorder_, horder_, n * sizeof(int), cudaMemcpyHostToDevice, s));
+      if (a.ysrc) q(cudaMemcpyAsync(dsrc_, hsrc_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
+      if (a.dpdt) q(cudaMemcpyAsync(dde_, hde_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+      if (a.esrc)
+        q(cudaMemcpyAsync(dde_ + cap_, hde_ + cap_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+      if (a.tdel_in)
+        q(cudaMemcpyAsync(dde_ + 2 * cap_, hde_ + 2 * cap_, n * sizeof(double),
+                          cudaMemcpyHostToDevice, s));
+      q(cudaMemsetAsync(dhead_, 0, sizeof(int), s));
+      q(cudaEventRecordWithFlags(ev0_, s, cudaEventRecordExternal));  // a timing node in the graph
+      q(method == 1 ? launch_integrate_dense(m, io, a, dthreads, dctas, spill, s)
+                    : launch_integrate(m, lud_, io, a, W, ctas, rop_smem, s));
+      q(cudaEventRecordWithFlags(ev1_, s, cudaEventRecordExternal));
+      q(cudaMemcpyAsync(hT_, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+      q(cudaMemcpyAsync(hP_, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+      q(cudaMemcpyAsync(hY_, dY_, (size_t)n * S * sizeof(double), cudaMemcpyDeviceToHost, s));
+      q(cudaMemcpyAsync(hstats_, dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s));
+      if (a.t_ign) q(cudaMemcpyAsync(hign_, dign_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+      cudaGraph_t g = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(s, &g);
+      if (ce == cudaSuccess) ce = ee;
+      if (ce == cudaSuccess) ce = cudaGraphInstantiate(&graph_, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (ce != cudaSuccess) {
+        graph_ = nullptr;
+        last_error = std::string("graph capture: ") + cudaGetErrorString(ce);
+        return -1;
+      }
+      graph_key_ = key;
+      ++graph_captures;
+    }
+    if ((e = cudaGraphLaunch(graph_, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+      last_error = std::string("integration: ") + cudaGetErrorString(e);
       return -1;
     }
-    graph_key_ = key;
-    ++graph_captures;
+    ++graph_launches;
   }
-  if ((e = cudaGraphLaunch(graph_, s)) != cudaSuccess || (e = cudaStreamSynchronize(s)) != cudaSuccess) {
-    last_error = std::string("integration: ") + cudaGetErrorString(e);
-    return -1;
-  }
-  ++graph_launches;
   std::memcpy(T, hT_, n * sizeof(double));
   std::memcpy(P, hP_, n * sizeof(double));
   const ReactorStats *st = hstats_;
   float ms = 0.f;
-  if (cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) {
+  if (cudaEventElapsedTime(&ms, ev0_, ev1_) != cudaSuccess) {  // (the callback path records them too)
     ms = 0.f;
     (void)cudaGetLastError();  // timing only: leave no error for the next launch check
   }

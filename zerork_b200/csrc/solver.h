@@ -42,6 +42,22 @@ struct SolveOptions {
   bool abstol_dens = false;          // species absolute tolerances / molar density
 };
 
+// The plugin's per-step callback (zerork_callback_fn of zerork_cfd_plugin.h):
+// called after every accepted step of every reactor, and once more at the
+// first crossing of the ignition temperature, with the reactor's id
+// (reactor_ids[k], or the reactor's index k where the reference passes its
+// position in the cost-sorted order, zerork_reactor_manager.cpp:1105-1108),
+// the reference's call counter, the time from the call's start, the time
+// since the previous call, the state y = [Y, T/Tref] and its derivative; a
+// nonzero return ends that reactor's call there (solver_cvode.cpp:247-262).
+// Calls come reactor by reactor in index order after the batch integrated.
+struct StepCallback {
+  int (*fn)(int reactor_id, int steps, double time, double dt, const double *y, const double *dy,
+            void *data) = nullptr;
+  void *data = nullptr;
+  const int *reactor_ids = nullptr;
+};
+
 struct SolveStatsTotals {
   long nsteps = 0, nrej = 0, nnewt = 0, njac = 0, nlu = 0, nrhs = 0, nkry = 0;
   int nfailed = 0;
@@ -68,11 +84,14 @@ class ReactorSolver {
             int stride, double *cost, double *gpu_time, double *temp_delta,
             double temp_threshold, std::vector<ReactorStats> *stats, SolveStatsTotals *tot,
             const double *ysrc = nullptr, double *t_ign = nullptr, const double *dpdt = nullptr,
-            const double *esrc = nullptr);
+            const double *esrc = nullptr, const StepCallback *cb = nullptr);
   std::string last_error;
 
  private:
   cudaError_t reserve(int n, bool fp32);
+  cudaError_t solve_with_callback(int method, const IntegOpts &io, IntegArgs a, int dthreads,
+                                  int dctas, int spill, int W, int ctas, bool rop_smem, int n,
+                                  double dt, const StepCallback &cb);
   MechTables tables_;
   JacPattern pat_;
   LUSymbolic lus_;
@@ -99,6 +118,11 @@ class ReactorSolver {
   // one CUDA graph per call configuration: H2D copies, queue reset, the
   // persistent integration kernel between two timing events, D2H copies
   cudaGraphExec_t graph_ = nullptr;
+  // step-callback records (solve with a StepCallback)
+  double *dcb_rec_ = nullptr;
+  int *dcb_cnt_ = nullptr, *dcb_stop_ = nullptr, *dcb_order_ = nullptr;
+  size_t dcb_bytes_ = 0;
+  int dcb_n_ = 0;
   std::vector<unsigned char> graph_key_;
  public:
   long graph_launches = 0, graph_captures = 0;

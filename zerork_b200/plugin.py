@@ -29,6 +29,10 @@ class PluginError(RuntimeError):
 
 _bound = False
 
+# zerork_callback_fn (applications/cfd_plugin/zerork_cfd_plugin.h:44-46)
+CALLBACK = C.CFUNCTYPE(C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                       C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p)
+
 
 def plugin_lib():
     global _bound
@@ -48,6 +52,8 @@ def plugin_lib():
         L.zerork_reactor_get_double_option.argtypes = [cp, C.POINTER(C.c_double), vp]
         L.zerork_reactor_get_string_option.argtypes = [cp, C.POINTER(C.c_char_p), C.c_int, vp]
         L.zerork_reactor_set_reactor_ids.argtypes = [vp, vp]
+        L.zerork_reactor_set_callback_fn.argtypes = [CALLBACK, vp, vp]
+        L.zrk_plugin_num_species.argtypes = [vp]
         L.zerork_reactor_free.argtypes = [vp]
         L.zrk_plugin_last_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_float)]
         L.zrk_plugin_set_predictor.argtypes = [vp, vp, vp, vp, vp, vp]
@@ -130,6 +136,30 @@ class Plugin:
         self._keep[field] = a
         self.check(self.L.zerork_reactor_set_aux_field_pointer(FIELDS[field], a.ctypes.data, self.h),
                    f"aux {field}")
+        return a
+
+    def set_callback(self, fn):
+        """Per-step callback fn(reactor_id, steps, time, dt, y, dy) -> int,
+        y and dy float64 arrays of nsp + 1 (mass fractions, T / Tref) valid
+        during the call; a nonzero return ends that reactor's integration at
+        that step (zerork_reactor_set_callback_fn, solver_cvode.cpp:247-257)."""
+        nv = [None]
+
+        def tramp(rid, steps, t, dt, y, dy, _data):
+            if nv[0] is None:
+                nv[0] = self.L.zrk_plugin_num_species(self.h) + 1
+            n = nv[0]
+            return int(fn(rid, steps, t, dt, np.ctypeslib.as_array(y, (n,)),
+                          np.ctypeslib.as_array(dy, (n,))))
+
+        cfn = CALLBACK(tramp)
+        self._keep["callback"] = cfn
+        self.check(self.L.zerork_reactor_set_callback_fn(cfn, None, self.h), "set_callback_fn")
+
+    def set_reactor_ids(self, ids):
+        a = np.ascontiguousarray(ids, dtype=np.int32)
+        self._keep["reactor_ids"] = a
+        self.check(self.L.zerork_reactor_set_reactor_ids(a.ctypes.data, self.h), "set_reactor_ids")
         return a
 
     def solve(self, dt, T, P, Y, n_cycle=0, time=0.0, raise_on_fail=True):
