@@ -553,7 +553,7 @@ struct Consts {
   double gam[kMaxOrder + 2], alp[kMaxOrder + 2], econ[kMaxOrder + 2];
 };
 
-__device__ void make_consts(Consts &b) {
+__host__ __device__ inline void make_consts(Consts &b) {
   const double kap[kMaxOrder + 1] = {0.0, -0.1850, -1.0 / 9.0, -0.0823, -0.0415, 0.0};
   for (int k = 0; k <= kMaxOrder + 1; ++k) {
     double g = 0.0;
@@ -905,9 +905,11 @@ __device__ __forceinline__ int attempt_cta(const DevMech &m, const IntegOpts &o,
         const double dn = sqrt(block_sum(a, s.red) / n);
         if (dnorm_old > 0.0) crate = fmax(0.3 * crate, dn / dnorm_old);
         // from a learned starting iterate, convergence is only declared on
-        // a contraction measured in this step (two iterations at least): the
-        // carried rate estimate describes the polynomial predictor's start
-        if (!(use_pred && it == 0) && bc.econ[q] * dn * fmin(1.0, crate) <= o.nlscoef) {
+        // the last correction itself (two iterations at least): neither the
+        // carried rate estimate (the polynomial predictor's start) nor one
+        // measured from a large first correction bounds the remaining error
+        const double dconv = use_pred ? dn : dn * fmin(1.0, crate);
+        if (!(use_pred && it == 0) && bc.econ[q] * dconv <= o.nlscoef) {
           conv = true;
           ++it;
           break;

@@ -1,6 +1,7 @@
 // plugin.cpp -- zerork_reactor_* C ABI (include/zerork_cfd_plugin.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -208,6 +209,7 @@ static zrk::SolveOptions options_of(zerork_handle_impl *h) {
   o.sort_reactors = I["sort_reactors"] != 0;
   o.warps_per_cta = I["gpu_warps_per_cta"];
   o.method = I["gpu_method"];
+  o.group_max = std::max(1, I["n_reactors_max"]);
   o.threads = I["gpu_threads"];
   o.pred = h->pred;
   o.dT_ign = D["delta_temperature_ignition"];
@@ -364,6 +366,17 @@ int zrk_plugin_krylov_iterations(zerork_handle h, long *iterations) {
 
 int zrk_plugin_num_species(zerork_handle h) {
   return (h && h->solver) ? h->solver->nsp() : -1;
+}
+
+int zrk_plugin_group_stats(zerork_handle h, long *out5) {
+  if (!h) return ZRK_ERR_INVALID_HANDLE;
+  if (!out5) return ZRK_ERR_INVALID_POINTER;
+  out5[0] = h->last.groups;
+  out5[1] = h->last.group_steps;
+  out5[2] = h->last.group_newton;
+  out5[3] = h->last.launches;
+  out5[4] = h->last.syncs;
+  return ZRK_OK;
 }
 
 int zrk_plugin_graph_stats(zerork_handle h, long *captures, long *launches) {

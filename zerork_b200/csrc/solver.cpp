@@ -1,6 +1,8 @@
 // solver.cpp -- see solver.h.
 #include "solver.h"
 
+#include "integrator_group.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -57,6 +59,7 @@ ReactorSolver::~ReactorSolver() {
   cudaFree(dcb_rec_); cudaFree(dcb_cnt_); cudaFree(dcb_stop_); cudaFree(dcb_order_);
   cudaFree(dT_); cudaFree(dP_); cudaFree(dY_); cudaFree(dv_); cudaFree(dstate_); cudaFree(dlu_);
   cudaFree(dstats_); cudaFree(dorder_); cudaFree(dhead_); cudaFree(drop_);
+  cudaFree(dgrp_); cudaFree(dpart_); cudaFreeHost(hpart_);
   if (ev0_) cudaEventDestroy(ev0_);
   if (ev1_) cudaEventDestroy(ev1_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -316,6 +319,22 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     }
   int method = o.method;
   if (method == 0) method = spill >= 0 ? 1 : 2;
+  if (method == 3) {  // the plain FP64 group path supports the reference's basic reactor
+    const char *why = nullptr;
+    if (m.nsp + 1 > kDenseMaxN) why = "more than 255 species";
+    else if (o.lu_fp32) why = "lu_fp32";
+    else if (o.pred.enabled) why = "a learned predictor";
+    else if (esrc) why = "E_SRC";
+    else if (cb && cb->fn) why = "a step callback";
+    else if (o.stop_after_ignition && o.dT_ign > 0.0) why = "stop_after_ignition";
+    if (why) {
+      last_error = std::string("gpu_method 3 (plain FP64 group path) does not support ") + why;
+      return -1;
+    }
+  } else if (method < 0 || method > 3) {
+    last_error = "gpu_method must be 0, 1, 2 or 3";
+    return -1;
+  }
   if (method == 1 && spill < 0) {
     last_error = "dense block does not fit in shared memory";
     return -1;
@@ -419,7 +438,68 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     a.state_stride = m.nnz;
   }
   const bool with_cb = cb && cb->fn;
-  if (with_cb) {
+  GroupCounters gcnt;
+  if (method == 3) {
+    // host-driven, kernel by kernel (the reference GPU path's structure):
+    // not captured in a graph
+    const int gmax = std::min(std::max(1, o.group_max), n);
+    const size_t slot_bytes = group_slot_doubles(m) * sizeof(double);
+    const size_t need = (size_t)gmax * slot_bytes;
+    if (need > dgrp_bytes_) {
+      cudaFree(dgrp_);
+      dgrp_ = nullptr;
+      dgrp_bytes_ = 0;
+      if ((e = cudaMalloc(&dgrp_, need)) != cudaSuccess) {
+        last_error = "group workspace allocation";
+        return -1;
+      }
+      dgrp_bytes_ = need;
+    }
+    if (gmax > part_cap_) {
+      cudaFree(dpart_);
+      cudaFreeHost(hpart_);
+      dpart_ = hpart_ = nullptr;
+      part_cap_ = 0;
+      if ((e = cudaMalloc(&dpart_, (size_t)gmax * 6 * sizeof(double))) != cudaSuccess ||
+          (e = cudaMallocHost(&hpart_, (size_t)gmax * 6 * sizeof(double))) != cudaSuccess) {
+        last_error = "group partial-sum allocation";
+        return -1;
+      }
+      part_cap_ = gmax;
+    }
+    int threads = o.threads;
+    if (threads <= 0) {
+      const int work = std::max(m.nsp + 1, m.nrxn / 2);
+      threads = 32;
+      while (threads < work && threads < 512) threads *= 2;
+    }
+    cudaError_t ce = cudaSuccess;
+    auto q = [&](cudaError_t r) {
+      if (ce == cudaSuccess) ce = r;
+    };
+    q(cudaMemcpyAsync(dT_, hT_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaMemcpyAsync(dP_, hP_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaMemcpyAsync(dY_, hY_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaMemcpyAsync(dorder_, horder_, n * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (a.ysrc) q(cudaMemcpyAsync(dsrc_, hsrc_, (size_t)n * S * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (a.dpdt) q(cudaMemcpyAsync(dde_, hde_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (a.tdel_in)
+      q(cudaMemcpyAsync(dde_ + 2 * cap_, hde_ + 2 * cap_, n * sizeof(double), cudaMemcpyHostToDevice, s));
+    q(cudaEventRecord(ev0_, s));
+    if (ce == cudaSuccess)
+      q(integrate_group(m, io, a, dorder_, gmax, threads, dgrp_, dpart_, hpart_, s, &gcnt));
+    q(cudaEventRecord(ev1_, s));
+    q(cudaMemcpyAsync(hT_, dT_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaMemcpyAsync(hP_, dP_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaMemcpyAsync(hY_, dY_, (size_t)n * S * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaMemcpyAsync(hstats_, dstats_, n * sizeof(ReactorStats), cudaMemcpyDeviceToHost, s));
+    if (a.t_ign) q(cudaMemcpyAsync(hign_, dign_, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    q(cudaStreamSynchronize(s));
+    if (ce != cudaSuccess) {
+      last_error = std::string("group integration: ") + cudaGetErrorString(ce);
+      return -1;
+    }
+  } else if (with_cb) {
     if ((e = solve_with_callback(method, io, a, dthreads, dctas, spill, W, ctas, rop_smem, n, dt, *cb)) !=
         cudaSuccess) {
       last_error = std::string("integration with step callback: ") + cudaGetErrorString(e);
@@ -532,6 +612,11 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     tot->nfailed = nfail;
     tot->kernel_ms = ms;
     tot->method = method;
+    tot->groups = gcnt.groups;
+    tot->group_steps = gcnt.group_steps;
+    tot->group_newton = gcnt.group_newton;
+    tot->launches = gcnt.launches;
+    tot->syncs = gcnt.syncs;
   }
   return nfail;
 }

@@ -31,7 +31,9 @@ struct SolveOptions {
   bool lu_fp32 = false;
   bool sort_reactors = true;
   int warps_per_cta = 0;  // 0 = automatic
-  int method = 0;         // 0 automatic, 1 CTA dense block, 2 warp sparse LU
+  int method = 0;         // 0 automatic, 1 CTA dense block, 2 warp sparse LU, 3 the plain
+                          // FP64 group path (integrator_group.h)
+  int group_max = 1024;   // method 3: reactors per group (plugin option n_reactors_max)
   int threads = 0;        // CTA size of the dense method (0 = automatic)
   PredDev pred{};         // learned predictor (dense method only)
   double dT_ign = 0.0;    // delta_temperature_ignition (> 0: record ignition times)
@@ -63,6 +65,9 @@ struct SolveStatsTotals {
   int nfailed = 0;
   float kernel_ms = 0.f;
   int method = 0;
+  // method 3: groups, steps and Newton iterations of all groups, kernel
+  // launches and host synchronizations
+  long groups = 0, group_steps = 0, group_newton = 0, launches = 0, syncs = 0;
 };
 
 class ReactorSolver {
@@ -124,6 +129,10 @@ class ReactorSolver {
   size_t dcb_bytes_ = 0;
   int dcb_n_ = 0;
   std::vector<unsigned char> graph_key_;
+  // plain FP64 group path (method 3): per-reactor slots and partial sums
+  double *dgrp_ = nullptr, *dpart_ = nullptr, *hpart_ = nullptr;
+  size_t dgrp_bytes_ = 0;
+  int part_cap_ = 0;
  public:
   long graph_launches = 0, graph_captures = 0;
 };

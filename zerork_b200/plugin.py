@@ -59,6 +59,7 @@ def plugin_lib():
         L.zrk_plugin_set_predictor.argtypes = [vp, vp, vp, vp, vp, vp]
         L.zrk_plugin_graph_stats.argtypes = [vp, C.POINTER(C.c_long), C.POINTER(C.c_long)]
         L.zrk_plugin_krylov_iterations.argtypes = [vp, C.POINTER(C.c_long)]
+        L.zrk_plugin_group_stats.argtypes = [vp, C.POINTER(C.c_long)]
         L.zrk_plugin_autotune.argtypes = [vp, C.c_int, C.c_double, vp, vp, vp, C.POINTER(C.c_int),
                                           C.POINTER(C.c_float)]
         _bound = True
@@ -215,4 +216,8 @@ class Plugin:
         k = C.c_long()
         self.L.zrk_plugin_krylov_iterations(self.h, C.byref(k))
         d["nkry"] = k.value
+        g = (C.c_long * 5)()
+        self.L.zrk_plugin_group_stats(self.h, g)
+        for i, key in enumerate(("groups", "group_steps", "group_newton", "launches", "syncs")):
+            d[key] = int(g[i])
         return d
