@@ -56,6 +56,8 @@ def args_():
                    help="fraction of each config's reactor count (bounded calibration runs)")
     p.add_argument("--suite-pairs", type=int, default=1 << 20,
                    help="training pairs of the learned predictor in the suite")
+    p.add_argument("--plain-sample", type=int, default=1024,
+                   help="reactors the plain group path is timed on (a stratified sample)")
     p.add_argument("--integ-dt", type=float, default=2e-3,
                    help="integration interval per reactor in seconds (2 ms: the workload; "
                         "shorter only for bounded profiling captures)")
@@ -169,20 +171,73 @@ def cpu_reference(files, T, P, Y, budget_s=12.0, nthreads=None):
                       f"({kind} exp) + restated SetupJacobianSparse, {nthreads} OpenMP threads"}
 
 
-def reference_gpu_rates(files, T, P, Y, reps=5, n_max=1 << 18):
-    """The reference's own GPU rate path, mechanism_cuda::getReactionRates_CUDA_mr_dev
-    (src/zerork/mechanism_cuda.cu:150-156), compiled unmodified for sm_100a into
-    oracle/_ref/libzrk_ref_cuda.so, timed on the same (T, C) states beside this
-    repository's rates-from-concentrations kernel (zrk_rates_tc_dev, no limiter,
-    same outputs: net, create, destroy, rates of progress), in batches of n_max
-    reactors (the reference's nReactorsMax).  Both read T and C and write the
-    four outputs in the same species-major layout.  Returns None when the
-    library was not built."""
-    import ctypes as C
+def rates_tc_workload(files, T, P, Y, n_max=1 << 18):
+    """The (T, C) states of the rates-only comparison: the rate workload's
+    states as molar concentrations, species-major, in batches of n_max
+    reactors (the reference GPU mechanism's nReactorsMax)."""
     import torch
     import zerork_b200 as zb
+    pm = zb.Mechanism(*files, device=False)
+    mw = pm.table("mw")
+    rho = P / (8.314462618e3 * T * np.sum(Y / mw, axis=1))
+    conc = rho[:, None] * Y / mw
+    n = len(T)
+    nb = min(n, n_max)
+    dev = torch.device("cuda")
+    batches = []
+    for b0 in range(0, n - nb + 1, nb):
+        Tb = torch.from_numpy(np.ascontiguousarray(T[b0:b0 + nb])).to(dev)
+        Cb = torch.from_numpy(np.ascontiguousarray(conc[b0:b0 + nb].T)).to(dev)
+        batches.append((Tb, Cb))
+    return pm.nsp, pm.nstep, nb, batches
+
+
+def _time_rates_tc(fn, reps):
+    import torch
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def rates_only_b200(files, T, P, Y, reps=5):
+    """This repository's rates-from-concentrations kernel (zrk_rates_tc_dev:
+    net, create, destroy and rates of progress, no Jacobian, no limiter) on
+    the rates-only workload; the reference arm times the reference's own GPU
+    path (mechanism_cuda::getReactionRates_CUDA_mr_dev) on the same states."""
+    import torch
+    import zerork_b200 as zb
+    S, N, nb, batches = rates_tc_workload(files, T, P, Y)
+    pm = zb.Mechanism(*files)
+    kw = dict(dtype=torch.float64, device=torch.device("cuda"))
+    outs = [torch.empty((S, nb), **kw) for _ in range(3)] + [torch.empty((N, nb), **kw)]
+    L = zb.lib()
+
+    def step():
+        for Tb, Cb in batches:
+            zb.check(L.zrk_rates_tc_dev(pm.handle, nb, nb, zb._ptr(Tb), zb._ptr(Cb), None,
+                                        *[zb._ptr(o) for o in outs], None))
+    ms = _time_rates_tc(step, reps)
+    n = len(batches) * nb
+    return {"workload": f"rates from (T, C), no Jacobian: {S} species / {N} steps, {n} states "
+                        f"in batches of {nb}", "ms_per_step": ms, "states_per_s": n / (ms / 1e3),
+            "bytes_per_state": 8 * (1 + S + 3 * S + N)}
+
+
+def reference_gpu_rates(files, T, P, Y, reps=5):
+    """The reference's own GPU rate path, mechanism_cuda::getReactionRates_CUDA_mr_dev
+    (src/zerork/mechanism_cuda.cu:150-156), compiled unmodified for sm_100a into
+    oracle/_ref/libzrk_ref_cuda.so, on the rates-only workload of
+    rates_only_b200.  None when the library was not built or no GPU."""
+    import ctypes as C
+    import torch
     path = os.path.join(ROOT, "oracle", "_ref", "libzrk_ref_cuda.so")
-    if not os.path.exists(path):
+    if not os.path.exists(path) or not torch.cuda.is_available():
         return None
     L = C.CDLL(path)
     vp = C.c_void_p
@@ -190,83 +245,111 @@ def reference_gpu_rates(files, T, P, Y, reps=5, n_max=1 << 18):
     L.zrkref_cuda_load.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int]
     L.zrkref_cuda_free.argtypes = [vp]
     L.zrkref_cuda_rates.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp]
-    n = len(T)
-    nb = min(n, n_max)
+    S, N, nb, batches = rates_tc_workload(files, T, P, Y)
     h = L.zrkref_cuda_load(files[0].encode(), files[1].encode(), os.devnull.encode(), nb)
     if not h:
         return None
-    pm = zb.Mechanism(*files)
-    S, N = pm.nsp, pm.nstep
-    mw = pm.table("mw")
-    rho = P / (8.314462618e3 * T * np.sum(Y / mw, axis=1))
-    conc = rho[:, None] * Y / mw
-    dev = torch.device("cuda")
-    kw = dict(dtype=torch.float64, device=dev)
-    batches = []
-    for b0 in range(0, n - nb + 1, nb):
-        Tb = torch.from_numpy(np.ascontiguousarray(T[b0:b0 + nb])).to(dev)
-        Cb = torch.from_numpy(np.ascontiguousarray(conc[b0:b0 + nb].T)).to(dev)
-        batches.append((Tb, Cb))
+    kw = dict(dtype=torch.float64, device=torch.device("cuda"))
     outs = [torch.empty((S, nb), **kw) for _ in range(3)] + [torch.empty((N, nb), **kw)]
-    mine = [torch.empty((S, nb), **kw) for _ in range(3)] + [torch.empty((N, nb), **kw)]
     ptrs = [o.data_ptr() for o in outs]
 
-    def ref_step():
+    def step():
         for Tb, Cb in batches:
             L.zrkref_cuda_rates(h, nb, Tb.data_ptr(), Cb.data_ptr(), *ptrs)
-
-    def my_step():
-        for Tb, Cb in batches:
-            zb.check(zb.lib().zrk_rates_tc_dev(pm.handle, nb, nb, zb._ptr(Tb), zb._ptr(Cb), None,
-                                               *[zb._ptr(o) for o in mine], None))
-
-    res = {}
-    for name, fn in (("reference", ref_step), ("b200", my_step)):
-        fn()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(reps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        ms = e0.elapsed_time(e1) / reps
-        res[name] = {"ms_per_step": ms, "states_per_s": len(batches) * nb / (ms / 1e3)}
-    # the two agree (last batch): net rates at 1e-12 of create + destroy
-    net_r, cre_r, des_r = (o.cpu().numpy() for o in outs[:3])
-    net_m = mine[0].cpu().numpy()
-    scale = np.abs(cre_r) + np.abs(des_r)
+    ms = _time_rates_tc(step, reps)
     L.zrkref_cuda_free(h)
-    return {"workload": f"rates from (T, C), no Jacobian: {S} species / {N} steps, "
-                        f"{len(batches) * nb} states in batches of {nb} (nReactorsMax)",
-            "reference": res["reference"], "b200": res["b200"],
-            "ratio": res["reference"]["ms_per_step"] / res["b200"]["ms_per_step"],
-            "max_scaled_net_diff": float(np.max(np.abs(net_r - net_m) / np.maximum(scale, 1e-300))),
+    n = len(batches) * nb
+    return {"workload": f"rates from (T, C), no Jacobian: {S} species / {N} steps, {n} states "
+                        f"in batches of {nb} (nReactorsMax)", "ms_per_step": ms,
+            "states_per_s": n / (ms / 1e3),
             "source": "oracle/_ref/libzrk_ref_cuda.so (reference src/zerork CUDA sources, sm_100a)"}
 
 
-def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
+def _run_form(mf, tf, T, P, Y, dt, opts, net=None):
+    """One solve call of a form through the cfd_plugin API with host arrays;
+    wall time around the call (host copies included)."""
+    from zerork_b200.plugin import Plugin
+    p = Plugin(mf, tf, **opts)
+    if net is not None:
+        p.set_predictor(*net)
+    Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+    t0 = time.perf_counter()
+    rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
+    wall = time.perf_counter() - t0
+    st = p.last_stats()
+    p.close()
+    n = len(T)
+    res = {"value": n / wall, "unit": "reactors/s", "reactors": n, "wall_s": wall,
+           "kernel_ms": st["kernel_ms"], "status": rc, "failed": st["nfailed"],
+           "steps": st["nsteps"], "newton_per_step": st["nnewt"] / max(1, st["nsteps"]),
+           "rejected": st["nrej"], "factorizations": st["nlu"], "jacobians": st["njac"],
+           "krylov_per_newton": st["nkry"] / max(1, st["nnewt"]),
+           "h2d_bytes": int(T.nbytes + P.nbytes + Y.nbytes), "d2h_bytes": int(T.nbytes + P.nbytes + Y.nbytes)}
+    if st.get("groups"):
+        res.update(groups=st["groups"], group_steps=st["group_steps"], group_newton=st["group_newton"],
+                   launches=st["launches"], host_syncs=st["syncs"])
+    return res, (Tg, Yg)
+
+
+# The plain group path shares one step sequence among the reactors of a
+# group, so a group of reactors of uneven stiffness needs far more steps than
+# any of them alone: with the default 5000 steps per attempt every C3 group
+# fails (measured: 5 attempts x 5000 steps, all 512 reactors of a group
+# failed).  Its form runs with a step budget it can finish in.
+PLAIN_MAX_STEPS = 200000
+
+# The forms of the integration blocks.  "plain_fp64" is the plain FP64 GPU
+# path: the reference's GPU algorithm (one BDF per group of n_reactors_max =
+# 1024 reactors with a shared step size and WRMS norm, host-driven kernel by
+# kernel, gpu_method 3).  The batched forms run every reactor with its own
+# step control in one persistent graph-captured launch; "batched_fp32_learned"
+# is the chosen form (batched + FP32 preconditioner + learned predictor).
+FORMS = [("plain_fp64", dict(gpu_method=3, max_steps=PLAIN_MAX_STEPS), False),
+         ("batched_fp64", dict(), False),
+         ("batched_fp32", dict(lu_fp32=1), False),
+         ("batched_fp64_learned", dict(), True),
+         ("batched_fp32_learned", dict(lu_fp32=1), True)]
+
+
+def _plain_sample(n, n_plain):
+    """Reactor indices the plain group path is timed on: every k-th reactor
+    (a stratified sample of the same states)."""
+    if n_plain <= 0 or n_plain >= n:
+        return np.arange(n)
+    return np.arange(0, n, max(1, n // n_plain))[:n_plain]
+
+
+def _ratios(res):
+    base = res["plain_fp64"]["value"]
+    for form, _, _ in FORMS[1:]:
+        if form in res:
+            res[form]["over_plain"] = res[form]["value"] / base
+            res[form]["over_batched_fp64"] = res[form]["value"] / res["batched_fp64"]["value"]
+    if "batched_fp32_learned" in res:
+        res["chosen_over_plain"] = res["batched_fp32_learned"]["over_plain"]
+
+
+def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True, n_plain=1024):
     """Reactors integrated/s on the 160-species / 900-reaction mechanism (2 ms
     per reactor at rtol 1e-8, atol 1e-20) through the cfd_plugin API with host
-    arrays: the plain FP64 path (dense Newton inverse, direct solves) and the
-    FP32 form (single-precision inverse preconditioning an FP64 Krylov solve).
-    Each form is called twice on the same states; the second call, ordered by
-    the first call's per-reactor cost as the plugin does, is timed.  The CPU
-    oracle integrates a bounded sample of the same reactors on all host cores,
-    and its end states give the error of each GPU form."""
+    arrays, one solve call per form on the same states in index order: the
+    plain FP64 GPU path (the reference's group algorithm, timed on a
+    stratified sample of n_plain reactors, since it integrates group after
+    group at the same cost per reactor), the batched FP64 and FP32 forms, and
+    with the learned predictor (trained on the GPU on pairs the integrator
+    generates from other seeded states).  The CPU oracle integrates a bounded
+    sample of the same reactors on all host cores; its end states give the
+    error of each GPU form on that sample."""
     from zerork_b200 import mechgen
-    from zerork_b200.plugin import Plugin
     g = mechgen.generate(mechgen.SPECS["c3_160"])
     out = {"metric": "reactors integrated/s at rtol 1e-8", "unit": "reactors/s",
            "workload": f"160 species / 900 reactions, {n_reactors} constant-volume reactors "
                        "(T U[700,2500] K, P U[1,100] atm, 1-4 fuel-like species), "
-                       f"{dt * 1e3:g} ms each, rtol 1e-8, atol 1e-20"}
+                       f"{dt * 1e3:g} ms each, rtol 1e-8, atol 1e-20, one call per form, index order"}
     with tempfile.TemporaryDirectory() as d:
         mf, tf = g.write(d)
         T, P, Y = mechgen.reactor_states(g, n_reactors, "c3", seed=11)
-        # learned predictor: pairs from the integrator on other seeded states,
-        # trained on the GPU by the library's own kernels
-        forms = [("plain_fp64", 0, False), ("fp32_krylov", 1, False)]
+        net = None
         if learned:
             from zerork_b200 import predictor as pr
             t0 = time.perf_counter()
@@ -274,45 +357,26 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
             Xp, Tp = pr.generate_pairs(mf, tf, T0, P0, Y0, rounds=64, seed=5)
             t_gen = time.perf_counter() - t0
             t0 = time.perf_counter()
-            net, xs, ts, hist = pr.train(Xp, Tp, epochs=12, batch=1024, lr=1e-3)
-            t_train = time.perf_counter() - t0
-            out["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen, "train_s": t_train,
+            mlp, xs, ts, hist = pr.train(Xp, Tp, epochs=12, batch=1024, lr=1e-3)
+            net = (mlp, xs, ts)
+            out["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen,
+                                        "train_s": time.perf_counter() - t0,
                                         "loss_first_last": [hist[0], hist[-1]],
                                         "network": "163 -> 3 x 256 SiLU -> 161, BF16 weights, "
                                                    "FP32 accumulation"}
-            forms.append(("fp64_learned", 0, True))
         ends = {}
-        for name, fp32, use_net in forms:
-            p = Plugin(mf, tf, lu_fp32=fp32)
-            if use_net:
-                p.set_predictor(net, xs, ts)
-            cost = p.set_aux_field("COST", np.zeros(n_reactors))
-            Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
-            p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
-            Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
-            t0 = time.perf_counter()
-            rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
-            wall = time.perf_counter() - t0
-            st = p.last_stats()
-            ends[name] = (Tg, Yg)
-            out[name] = {"value": n_reactors / wall, "wall_s": wall, "kernel_ms": st["kernel_ms"],
-                         "status": rc, "failed": st["nfailed"], "steps": st["nsteps"],
-                         "newton_iters": st["nnewt"], "rejected": st["nrej"],
-                         "factorizations": st["nlu"], "jacobians": st["njac"],
-                         "newton_per_step": st["nnewt"] / max(1, st["nsteps"]),
-                         "krylov_per_newton": st["nkry"] / max(1, st["nnewt"]),
-                         "max_reactor_steps": int(np.max(np.abs(cost))),
-                         "mean_reactor_steps": float(np.mean(np.abs(cost))),
-                         "h2d_bytes": int(T.nbytes + P.nbytes + Y.nbytes),
-                         "d2h_bytes": int(T.nbytes + P.nbytes + Y.nbytes)}
-            p.close()
-        out["fp32_over_plain"] = out["fp32_krylov"]["value"] / out["plain_fp64"]["value"]
-        if learned:
-            out["learned_over_plain"] = out["fp64_learned"]["value"] / out["plain_fp64"]["value"]
-        out["note"] = ("wall time is set by the few reactors that reach max_steps (5000 per attempt, "
-                       "5 attempts) and run alone on one SM; which reactors fail differs between forms, "
-                       "so ratios between forms at this batch size mostly reflect that tail; compare "
-                       "newton_per_step, steps and mean_reactor_steps for the per-step effect")
+        for form, opts, use_net in FORMS:
+            if use_net and not learned:
+                continue
+            if form == "plain_fp64":
+                idx = _plain_sample(n_reactors, n_plain)
+                out[form], e = _run_form(mf, tf, T[idx], P[idx], Y[idx], dt, opts)
+                out[form]["sample"] = f"every {max(1, n_reactors // len(idx))}th reactor, {len(idx)} reactors"
+                ends[form] = (idx, e)
+            else:
+                out[form], e = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                ends[form] = (np.arange(n_reactors), e)
+        _ratios(out)
         if cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import zerork_b200 as zb
@@ -321,17 +385,19 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True):
             ot = _oracle_tables(pm, zo)
             nth = os.cpu_count() or 1
             m = min(n_reactors, 2 * nth)
+            idx = _plain_sample(n_reactors, n_plain)[:m]  # reactors every form integrated
             t0 = time.perf_counter()
-            To, Po, Yo, so = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth)
+            To, Po, Yo, so = ot.solve(T[idx], P[idx], Y[idx], dt, nthreads=nth)
             elapsed = time.perf_counter() - t0
             ok = so["status"] == 0
             out["cpu_oracle"] = {"value": m / elapsed, "unit": "reactors/s", "cores": nth, "kind": "port",
-                                 "sample": f"first {m} of the {n_reactors} reactors, restated "
+                                 "sample": f"{m} reactors of the plain path's sample, restated "
                                            "BDF/Newton with dense LU (FP64), one reactor per thread",
                                  "failed": int((~ok).sum())}
-            for name, (Tg, Yg) in ends.items():
-                out[name]["max_abs_dT_vs_oracle"] = float(np.abs(Tg[:m] - To)[ok].max())
-                out[name]["max_abs_dY_vs_oracle"] = float(np.abs(Yg[:m] - Yo)[ok].max())
+            for form, (ix, (Tg, Yg)) in ends.items():
+                pos = np.searchsorted(ix, idx)
+                out[form]["max_abs_dT_vs_oracle"] = float(np.abs(Tg[pos] - To)[ok].max())
+                out[form]["max_abs_dY_vs_oracle"] = float(np.abs(Yg[pos] - Yo)[ok].max())
     return out
 
 
@@ -344,21 +410,23 @@ INTEG_CONFIGS = {
 }
 
 
-def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None):
+def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None, n_plain=1024):
     """Every integration config through the cfd_plugin API (host arrays, one
-    solve call per form, reactors in the given order): plain FP64, the FP32
-    preconditioned form, the learned predictor, and FP32 + learned together.
-    Per form: reactors/s, solver counters, failed reactors, and the end-state
-    error on a sample against the CPU oracle (rtol 1e-8) and its
-    tight-tolerance run (rtol 1e-12, no per-step failure limits): the verdict
-    passes when every sampled reactor's |T - T_tight| is within 50 x the
-    oracle's own error (floored at 10 x the sample median) + 1e-5 T, and its
-    max |Y - Y_tight| within 50 x (same floor) + 1e-8, the bound of the test
-    suite (tests/test_integrator_gpu.py).  C5 trains the predictor network on
-    about `pairs` (state, interval, next state) pairs that the integrator
-    generates from other seeded states of the same mechanism."""
+    solve call per form, reactors in index order): the plain FP64 GPU path
+    (the reference's group algorithm, on a stratified sample of n_plain
+    reactors; dense-block mechanisms only, so not C4), the batched FP64 and
+    FP32 forms, and with the learned predictor (C1, C3, C5), the batched
+    FP32 + learned form being the chosen one.  Per form: reactors/s, solver
+    counters, failed reactors, and the end-state error on a sample against
+    the CPU oracle (rtol 1e-8) and its tight-tolerance run (rtol 1e-12, no
+    per-step failure limits): the verdict passes when every sampled
+    reactor's |T - T_tight| is within 50 x the oracle's own error (floored at
+    10 x the sample median) + 1e-5 T, and its max |Y - Y_tight| within 50 x
+    (same floor) + 1e-8, the bound of the test suite
+    (tests/test_integrator_gpu.py).  C5 trains the predictor network on about
+    `pairs` (state, interval, next state) pairs that the integrator generates
+    from other seeded states of the same mechanism."""
     from zerork_b200 import mechgen
-    from zerork_b200.plugin import Plugin
     import zerork_b200 as zb
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import zrk_oracle as zo
@@ -373,9 +441,9 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None):
         with tempfile.TemporaryDirectory() as d:
             mf, tf = g.write(d)
             T, P, Y = mechgen.reactor_states(g, nr, "c3" if wl == "c5" else wl, seed=11)
-            net = xs = ts = None
-            forms = [("plain_fp64", 0, False), ("fp32", 1, False)]
-            if name in ("c1", "c3", "c5"):
+            net = None
+            learned = name in ("c1", "c3", "c5")
+            if learned:
                 from zerork_b200 import predictor as pr
                 t0 = time.perf_counter()
                 ng = max(64, min(4096, pairs // 64))
@@ -384,52 +452,55 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None):
                 Xp, Tp = pr.generate_pairs(mf, tf, T0, P0, Y0, rounds=rounds, seed=5)
                 t_gen = time.perf_counter() - t0
                 t0 = time.perf_counter()
-                net, xs, ts, hist = pr.train(Xp, Tp, epochs=8 if Xp.shape[0] > 300000 else 12,
+                mlp, xs, ts, hist = pr.train(Xp, Tp, epochs=8 if Xp.shape[0] > 300000 else 12,
                                              batch=4096, lr=1e-3)
+                net = (mlp, xs, ts)
                 res["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen,
                                             "train_s": time.perf_counter() - t0,
                                             "loss_first_last": [hist[0], hist[-1]]}
-                forms += [("fp64_learned", 0, True), ("fp32_learned", 1, True)]
+            dense = len(g.species) + 1 <= 256
+            sample = _plain_sample(nr, n_plain)
             ends = {}
-            for form, fp32, use_net in forms:
-                p = Plugin(mf, tf, lu_fp32=fp32)
-                if use_net:
-                    p.set_predictor(net, xs, ts)
-                Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
-                t0 = time.perf_counter()
-                rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
-                wall = time.perf_counter() - t0
-                st = p.last_stats()
-                ends[form] = (Tg, Yg)
-                res[form] = {"value": nr / wall, "unit": "reactors/s", "wall_s": wall,
-                             "kernel_ms": st["kernel_ms"], "status": rc, "failed": st["nfailed"],
-                             "steps": st["nsteps"], "newton_per_step": st["nnewt"] / max(1, st["nsteps"]),
-                             "rejected": st["nrej"], "factorizations": st["nlu"],
-                             "jacobians": st["njac"],
-                             "krylov_per_newton": st["nkry"] / max(1, st["nnewt"])}
-                p.close()
-            base = res["plain_fp64"]["value"]
-            for form, _, _ in forms[1:]:
-                res[form]["over_plain"] = res[form]["value"] / base
+            for form, opts, use_net in FORMS:
+                if (use_net and not learned) or (form == "plain_fp64" and not dense):
+                    continue
+                if form == "plain_fp64":
+                    res[form], e = _run_form(mf, tf, T[sample], P[sample], Y[sample], dt, opts)
+                    res[form]["sample"] = f"every {max(1, nr // len(sample))}th reactor, {len(sample)} reactors"
+                    ends[form] = (sample, e)
+                else:
+                    res[form], e = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                    ends[form] = (np.arange(nr), e)
+            if "plain_fp64" in res:
+                _ratios(res)
+            else:
+                res["note"] = ("the plain group path needs the dense Newton block (at most 255 "
+                               "species); this mechanism runs on the batched sparse path only")
+                for form in list(res):
+                    if form.startswith("batched_") and form != "batched_fp64":
+                        res[form]["over_batched_fp64"] = res[form]["value"] / res["batched_fp64"]["value"]
             # end-state error on a sample against the oracle and its tight run
             pm = zb.Mechanism(mf, tf, device=False)
             ot = _oracle_tables(pm, zo)
             m = min(nr, msamp)
+            idx = sample[:m]
             t0 = time.perf_counter()
-            To, Po, Yo, so = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth)
+            To, Po, Yo, so = ot.solve(T[idx], P[idx], Y[idx], dt, nthreads=nth)
             t_oracle = time.perf_counter() - t0
-            Tt, Pt, Yt, stt = ot.solve(T[:m], P[:m], Y[:m], dt, nthreads=nth, rtol=1e-12,
+            Tt, Pt, Yt, stt = ot.solve(T[idx], P[idx], Y[idx], dt, nthreads=nth, rtol=1e-12,
                                        atol=1e-24, max_steps=400000, fail_caps=0)
             ok = (so["status"] == 0) & (stt["status"] == 0)
             res["cpu_oracle"] = {"value": m / t_oracle, "unit": "reactors/s", "cores": nth,
-                                 "kind": "port", "sample": f"first {m} reactors", "failed": int((~ok).sum())}
+                                 "kind": "port", "sample": f"{m} reactors of the plain path's sample",
+                                 "failed": int((~ok).sum())}
             eo_T = np.abs(To - Tt)[ok]
             eo_Y = np.max(np.abs(Yo - Yt), axis=1)[ok]
             fT = 10 * np.median(eo_T) if eo_T.size else 0.0
             fY = 10 * np.median(eo_Y) if eo_Y.size else 0.0
-            for form, (Tg, Yg) in ends.items():
-                eg_T = np.abs(Tg[:m] - Tt)[ok]
-                eg_Y = np.max(np.abs(Yg[:m] - Yt), axis=1)[ok]
+            for form, (ix, (Tg, Yg)) in ends.items():
+                pos = np.searchsorted(ix, idx)
+                eg_T = np.abs(Tg[pos] - Tt)[ok]
+                eg_Y = np.max(np.abs(Yg[pos] - Yt), axis=1)[ok]
                 bound_T = 50 * np.maximum(eo_T, fT) + 1e-5 * Tt[ok]
                 bound_Y = 50 * np.maximum(eo_Y, fY) + 1e-8
                 res[form]["max_abs_dT_vs_tight"] = float(eg_T.max()) if eg_T.size else None
@@ -437,6 +508,7 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None):
                 res[form]["oracle_max_abs_dT_vs_tight"] = float(eo_T.max()) if eo_T.size else None
                 res[form]["within_tolerance"] = bool(np.all(eg_T <= bound_T) and np.all(eg_Y <= bound_Y))
         out[name] = res
+        print(json.dumps({name: res}), flush=True)
     return out
 
 
@@ -485,6 +557,12 @@ def run_reference_arm(a, rank, world):
                                            " + restated SetupJacobianSparse"},
                 "e2e": {"value": v, "unit": "states/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
+        # the reference's own GPU rate path (rates only) on the full state set
+        try:
+            gT, gP, gY = make_workload(d, a.states, seed=7)[2:]
+            line["reference_gpu"] = reference_gpu_rates(files, gT, gP, gY)
+        except Exception as ex:  # no GPU on this host: the CPU line stands alone
+            line["reference_gpu"] = {"unavailable": str(ex)[:200]}
         print(json.dumps(line))
 
 
@@ -498,7 +576,7 @@ def main():
         return
     if a.integration_suite:
         res = integration_suite([x for x in a.integration_suite.split(",") if x], a.suite_scale,
-                                a.suite_pairs)
+                                a.suite_pairs, n_plain=a.plain_sample)
         print(json.dumps({"integration_suite": res}))
         return
     import torch
@@ -612,13 +690,14 @@ def main():
         e2e = {"value": world * n / dt, "unit": "states/s",
                "h2d_bytes_per_step": int(Th.nbytes + Ph.nbytes + Yh.nbytes),
                "d2h_bytes_per_step": int(Wh.nbytes + Jh.nbytes), "steps": e2e_steps}
+    rates_only = rates_only_b200(files, T, P, Y) if rank == 0 else None
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_reference(files, T, P, Y)
     integ = None
     if rank == 0 and world == 1 and a.reactors > 0:
         integ = integration_bench(a.reactors, cpu=not a.no_cpu, dt=a.integ_dt,
-                                  learned=not a.no_learned)
+                                  learned=not a.no_learned, n_plain=a.plain_sample)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "states/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
@@ -629,7 +708,8 @@ def main():
                            "global_states": world * n, "parallelism": f"shard{world}",
                            "l2": "inputs 445 MB + outputs 15 GB per step exceed L2; no flush",
                            "launch": pm.get_launch(), "autotune_sample_ms": tuned_ms},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "integration": integ,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "rates_only": rates_only,
+                "integration": integ,
                 "gpu_launches": a.steps, "clocks": clk.summary()}
         print(json.dumps(line))
     if world > 1:
