@@ -265,18 +265,28 @@ def reference_gpu_rates(files, T, P, Y, reps=5):
             "source": "oracle/_ref/libzrk_ref_cuda.so (reference src/zerork CUDA sources, sm_100a)"}
 
 
-def _run_form(mf, tf, T, P, Y, dt, opts, net=None):
-    """One solve call of a form through the cfd_plugin API with host arrays;
-    wall time around the call (host copies included)."""
+def _run_form(mf, tf, T, P, Y, dt, opts, net=None, cost=None, warm=True):
+    """A form through the cfd_plugin API with host arrays, as a CFD code calls
+    it step after step: a first call (untimed, warm=True) fills the COST field
+    and the timed call takes the reactors in that cost order (the plugin's
+    sort_reactors); cost, if given, is the COST field to start from instead.
+    Wall time around the timed call (host copies included).  Returns the
+    form's record, the end states and the per-reactor cost (negative for a
+    failed reactor)."""
     from zerork_b200.plugin import Plugin
     p = Plugin(mf, tf, **opts)
     if net is not None:
         p.set_predictor(*net)
+    c = p.set_aux_field("COST", np.zeros(len(T)) if cost is None else np.array(cost, dtype=np.float64))
+    if warm:
+        Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
+        p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
     Tg, Pg, Yg = T.copy(), P.copy(), Y.copy()
     t0 = time.perf_counter()
     rc = p.solve(dt, Tg, Pg, Yg, raise_on_fail=False)
     wall = time.perf_counter() - t0
     st = p.last_stats()
+    cost_out = np.array(c)
     p.close()
     n = len(T)
     res = {"value": n / wall, "unit": "reactors/s", "reactors": n, "wall_s": wall,
@@ -287,8 +297,8 @@ def _run_form(mf, tf, T, P, Y, dt, opts, net=None):
            "h2d_bytes": int(T.nbytes + P.nbytes + Y.nbytes), "d2h_bytes": int(T.nbytes + P.nbytes + Y.nbytes)}
     if st.get("groups"):
         res.update(groups=st["groups"], group_steps=st["group_steps"], group_newton=st["group_newton"],
-                   launches=st["launches"], host_syncs=st["syncs"])
-    return res, (Tg, Yg)
+                   launches=st["launches"], host_syncs=st["syncs"], group_status=st["group_status"])
+    return res, (Tg, Yg), cost_out
 
 
 # The plain group path shares one step sequence among the reactors of a
@@ -317,6 +327,19 @@ def _plain_sample(n, n_plain):
     if n_plain <= 0 or n_plain >= n:
         return np.arange(n)
     return np.arange(0, n, max(1, n // n_plain))[:n_plain]
+
+
+def _plain_pick(n, n_plain, cost):
+    """The plain path's reactors: a stratified sample of n_plain reactors
+    without those the batched FP64 path failed (one failed reactor fails its
+    whole group on the plain path), taken in the batched FP64 path's cost
+    order (reactors of similar stiffness share a group: the order most
+    favourable to a shared step size)."""
+    ok = np.flatnonzero(cost > 0)
+    idx = ok[_plain_sample(len(ok), n_plain)]
+    note = (f"{len(idx)} reactors: every {max(1, len(ok) // len(idx))}th of the {len(ok)} reactors the "
+            f"batched FP64 path integrated ({n - len(ok)} failed there), in its cost order")
+    return np.sort(idx), note
 
 
 def _ratios(res):
@@ -364,17 +387,19 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True, n_plain=1024)
                                         "loss_first_last": [hist[0], hist[-1]],
                                         "network": "163 -> 3 x 256 SiLU -> 161, BF16 weights, "
                                                    "FP32 accumulation"}
-        ends = {}
-        for form, opts, use_net in FORMS:
+        ends, cost = {}, None
+        for form, opts, use_net in FORMS[1:] + FORMS[:1]:  # the plain path last
             if use_net and not learned:
                 continue
             if form == "plain_fp64":
-                idx = _plain_sample(n_reactors, n_plain)
-                out[form], e = _run_form(mf, tf, T[idx], P[idx], Y[idx], dt, opts)
-                out[form]["sample"] = f"every {max(1, n_reactors // len(idx))}th reactor, {len(idx)} reactors"
+                idx, note = _plain_pick(n_reactors, n_plain, cost)
+                out[form], e, _ = _run_form(mf, tf, T[idx], P[idx], Y[idx], dt, opts, cost=cost[idx], warm=False)
+                out[form]["sample"] = note
                 ends[form] = (idx, e)
             else:
-                out[form], e = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                out[form], e, c = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                if form == "batched_fp64":
+                    cost = c
                 ends[form] = (np.arange(n_reactors), e)
         _ratios(out)
         if cpu:
@@ -385,7 +410,7 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True, n_plain=1024)
             ot = _oracle_tables(pm, zo)
             nth = os.cpu_count() or 1
             m = min(n_reactors, 2 * nth)
-            idx = _plain_sample(n_reactors, n_plain)[:m]  # reactors every form integrated
+            idx = ends["plain_fp64"][0][:m]  # reactors every form integrated
             t0 = time.perf_counter()
             To, Po, Yo, so = ot.solve(T[idx], P[idx], Y[idx], dt, nthreads=nth)
             elapsed = time.perf_counter() - t0
@@ -459,18 +484,22 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None, n_plain=102
                                             "train_s": time.perf_counter() - t0,
                                             "loss_first_last": [hist[0], hist[-1]]}
             dense = len(g.species) + 1 <= 256
-            sample = _plain_sample(nr, n_plain)
-            ends = {}
-            for form, opts, use_net in FORMS:
+            ends, cost = {}, None
+            for form, opts, use_net in FORMS[1:] + FORMS[:1]:  # the plain path last
                 if (use_net and not learned) or (form == "plain_fp64" and not dense):
                     continue
                 if form == "plain_fp64":
-                    res[form], e = _run_form(mf, tf, T[sample], P[sample], Y[sample], dt, opts)
-                    res[form]["sample"] = f"every {max(1, nr // len(sample))}th reactor, {len(sample)} reactors"
+                    sample, note = _plain_pick(nr, n_plain, cost)
+                    res[form], e, _ = _run_form(mf, tf, T[sample], P[sample], Y[sample], dt, opts,
+                                                cost=cost[sample], warm=False)
+                    res[form]["sample"] = note
                     ends[form] = (sample, e)
                 else:
-                    res[form], e = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                    res[form], e, c = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                    if form == "batched_fp64":
+                        cost = c
                     ends[form] = (np.arange(nr), e)
+            sample = ends["plain_fp64"][0] if "plain_fp64" in ends else np.flatnonzero(cost > 0)
             if "plain_fp64" in res:
                 _ratios(res)
             else:

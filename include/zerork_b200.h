@@ -168,11 +168,12 @@ int zrk_plugin_krylov_iterations(struct zerork_handle_impl *h, long *iterations)
 /* Counters of the last solve on the plain FP64 group path (option
  * gpu_method = 3, one BDF integration per group of n_reactors_max reactors
  * with a shared step size, as the reference GPU path integrates a batch with
- * one CVODE instance, zerork_reactor_manager.cpp:909-1054): out5 = {groups,
+ * one CVODE instance, zerork_reactor_manager.cpp:909-1054): out6 = {groups,
  * steps summed over the groups, Newton iterations summed over the groups,
- * kernel launches, host synchronizations}; zeros after a solve on another
- * method.  No counterpart in the reference. */
-int zrk_plugin_group_stats(struct zerork_handle_impl *h, long *out5);
+ * kernel launches, host synchronizations, the status of the first group that
+ * failed (0: none; the batched integrators' negative codes)}; zeros after a
+ * solve on another method.  No counterpart in the reference. */
+int zrk_plugin_group_stats(struct zerork_handle_impl *h, long *out6);
 
 /* Species count of the handle's loaded mechanism (the step callback's y and
  * dy hold nsp + 1 entries: mass fractions, then T / Tref), or -1 before

@@ -712,6 +712,7 @@ cudaError_t integrate_group(const DevMech &m, const IntegOpts &o, const IntegArg
       gc->groups++;
       gc->group_steps += drv.cnt.nsteps;
       gc->group_newton += drv.cnt.nnewt;
+      if (rc != 0 && gc->first_fail == 0) gc->first_fail = rc;
     }
     g0 += gs;
   }

@@ -13,6 +13,7 @@ namespace zrk {
 
 struct GroupCounters {
   long groups = 0, group_steps = 0, group_newton = 0, launches = 0, syncs = 0;
+  long first_fail = 0;  // status of the first group whose attempts all failed
 };
 
 // Doubles of device workspace per reactor of a group (the reactor's BDF

@@ -368,14 +368,15 @@ int zrk_plugin_num_species(zerork_handle h) {
   return (h && h->solver) ? h->solver->nsp() : -1;
 }
 
-int zrk_plugin_group_stats(zerork_handle h, long *out5) {
+int zrk_plugin_group_stats(zerork_handle h, long *out6) {
   if (!h) return ZRK_ERR_INVALID_HANDLE;
-  if (!out5) return ZRK_ERR_INVALID_POINTER;
-  out5[0] = h->last.groups;
-  out5[1] = h->last.group_steps;
-  out5[2] = h->last.group_newton;
-  out5[3] = h->last.launches;
-  out5[4] = h->last.syncs;
+  if (!out6) return ZRK_ERR_INVALID_POINTER;
+  out6[0] = h->last.groups;
+  out6[1] = h->last.group_steps;
+  out6[2] = h->last.group_newton;
+  out6[3] = h->last.launches;
+  out6[4] = h->last.syncs;
+  out6[5] = h->last.group_status;
   return ZRK_OK;
 }
 

@@ -617,6 +617,7 @@ int ReactorSolver::solve(const SolveOptions &o, int n, double dt, double *T, dou
     tot->group_newton = gcnt.group_newton;
     tot->launches = gcnt.launches;
     tot->syncs = gcnt.syncs;
+    tot->group_status = gcnt.first_fail;
   }
   return nfail;
 }

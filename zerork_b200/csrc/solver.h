@@ -68,6 +68,7 @@ struct SolveStatsTotals {
   // method 3: groups, steps and Newton iterations of all groups, kernel
   // launches and host synchronizations
   long groups = 0, group_steps = 0, group_newton = 0, launches = 0, syncs = 0;
+  long group_status = 0;  // status of the first failed group (0: none)
 };
 
 class ReactorSolver {

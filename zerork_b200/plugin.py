@@ -216,8 +216,9 @@ class Plugin:
         k = C.c_long()
         self.L.zrk_plugin_krylov_iterations(self.h, C.byref(k))
         d["nkry"] = k.value
-        g = (C.c_long * 5)()
+        g = (C.c_long * 6)()
         self.L.zrk_plugin_group_stats(self.h, g)
-        for i, key in enumerate(("groups", "group_steps", "group_newton", "launches", "syncs")):
+        for i, key in enumerate(("groups", "group_steps", "group_newton", "launches", "syncs",
+                                 "group_status")):
             d[key] = int(g[i])
         return d
