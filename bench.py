@@ -56,7 +56,7 @@ def args_():
                    help="fraction of each config's reactor count (bounded calibration runs)")
     p.add_argument("--suite-pairs", type=int, default=1 << 20,
                    help="training pairs of the learned predictor in the suite")
-    p.add_argument("--plain-sample", type=int, default=1024,
+    p.add_argument("--plain-sample", type=int, default=256,
                    help="reactors the plain group path is timed on (a stratified sample)")
     p.add_argument("--integ-dt", type=float, default=2e-3,
                    help="integration interval per reactor in seconds (2 ms: the workload; "
@@ -343,7 +343,15 @@ def _plain_pick(n, n_plain, cost):
 
 
 def _ratios(res):
+    """Throughput ratios over the plain path and over the batched FP64 form.
+    When the plain path failed (its group's every attempt), its reactors/s is
+    the sample over the time it ran before failing, an upper bound on its
+    rate, and the ratios over it are lower bounds."""
     base = res["plain_fp64"]["value"]
+    res["plain_fp64"]["finished"] = res["plain_fp64"]["failed"] == 0
+    if not res["plain_fp64"]["finished"]:
+        res["plain_fp64"]["note"] = ("the group integration failed after the steps shown; its value is "
+                                     "an upper bound on the plain path's rate, the ratios over it lower bounds")
     for form, _, _ in FORMS[1:]:
         if form in res:
             res[form]["over_plain"] = res[form]["value"] / base
@@ -727,6 +735,9 @@ def main():
     if rank == 0 and world == 1 and a.reactors > 0:
         integ = integration_bench(a.reactors, cpu=not a.no_cpu, dt=a.integ_dt,
                                   learned=not a.no_learned, n_plain=a.plain_sample)
+        # the small config (64 reactors, 10 species), where the plain group
+        # path finishes: every form with its end-state verdict
+        integ["c1"] = integration_suite(["c1"], pairs=1 << 16)["c1"]
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "states/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
