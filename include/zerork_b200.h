@@ -70,11 +70,16 @@ int zrk_mech_set_double_option(zrk_mech_t m, const char *name, double value);
 int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value);
 
 /* Tile mapping of the rate kernel: ts states per tile (8/16/32), v states
- * per thread (1/2/4), warps per CTA (1..16; 32 with v = 1), global_ws = 1 puts the per-tile
- * workspace in global scratch (grid CTAs; 0 = one CTA per tile).  ts = 0
- * restores the default mapping. */
-int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int global_ws, int grid);
-int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *global_ws, int *grid);
+ * per thread (1/2/4), warps per CTA (1..16; 32 with v = 1); flags bit 0
+ * (ZRK_LAUNCH_GLOBAL_WS) puts the per-tile workspace in global scratch (grid
+ * CTAs; 0 = one CTA per tile), bit 1 (ZRK_LAUNCH_STAGE_TABLES) copies the
+ * mechanism tables the kernel reads into each CTA's shared memory beside
+ * the workspace (rejected when the two do not fit).  ts = 0 restores the
+ * default mapping. */
+#define ZRK_LAUNCH_GLOBAL_WS 1
+#define ZRK_LAUNCH_STAGE_TABLES 2
+int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int flags, int grid);
+int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *flags, int *grid);
 
 /* Autotuner: times every valid (ts, v, warps) mapping on the caller's sample
  * (device arrays as for zrk_rates_jac_dev, outputs overwritten) and keeps the

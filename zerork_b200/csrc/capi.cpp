@@ -210,7 +210,7 @@ int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value) {
   return ZRK_OK;
 }
 
-int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int global_ws, int grid) {
+int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int flags, int grid) {
   if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
   MechHandle *h = reinterpret_cast<MechHandle *>(m);
   if (!h->dev) return set_error(ZRK_ERR_NO_DEVICE, "handle has no device tables (zrk_mech_parse)");
@@ -222,23 +222,24 @@ int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int global_ws, i
   c.ts = ts;
   c.v = v;
   c.warps = warps;
-  c.global_ws = global_ws != 0;
+  c.global_ws = (flags & ZRK_LAUNCH_GLOBAL_WS) != 0;
+  c.stage = (flags & ZRK_LAUNCH_STAGE_TABLES) != 0;
   c.grid = grid;
-  if (!rates_jac_mapping_ok(c) || grid < 0)
+  if (!rates_jac_mapping_ok(c) || grid < 0 || (flags & ~3))
     return set_error(ZRK_ERR_INVALID_ARGUMENT, "bad launch mapping");
-  if (!c.global_ws && rates_jac_ws_bytes(h->dev->view(), c) > 227 * 1024)
-    return set_error(ZRK_ERR_INVALID_ARGUMENT, "workspace does not fit in shared memory");
+  if (rates_jac_smem_bytes(h->dev->view(), c) > 227 * 1024)
+    return set_error(ZRK_ERR_INVALID_ARGUMENT, "workspace and staged tables do not fit in shared memory");
   h->cfg = c;
   return ZRK_OK;
 }
 
-int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *global_ws, int *grid) {
+int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *flags, int *grid) {
   if (!m) return set_error(ZRK_ERR_INVALID_HANDLE, "null handle");
   MechHandle *h = reinterpret_cast<MechHandle *>(m);
   if (ts) *ts = h->cfg.ts;
   if (v) *v = h->cfg.v;
   if (warps) *warps = h->cfg.warps;
-  if (global_ws) *global_ws = h->cfg.global_ws ? 1 : 0;
+  if (flags) *flags = (h->cfg.global_ws ? ZRK_LAUNCH_GLOBAL_WS : 0) | (h->cfg.stage ? ZRK_LAUNCH_STAGE_TABLES : 0);
   if (grid) *grid = h->cfg.grid;
   return ZRK_OK;
 }
@@ -270,6 +271,9 @@ int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double
           c.global_ws = true;
           c.grid = 2 * sms;
         }
+        for (int stage = 0; stage < 2; ++stage) {
+        c.stage = stage != 0;
+        if (c.stage && rates_jac_smem_bytes(h->dev->view(), c) > 227 * 1024) continue;
         h->cfg = c;
         float t = 0.f;
         bool ok = true;
@@ -285,6 +289,7 @@ int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double
         if (ok && cudaGetLastError() == cudaSuccess && t < best_t) {
           best_t = t;
           best = c;
+        }
         }
       }
   cudaEventDestroy(e0);

@@ -16,8 +16,8 @@ const double kRu = 8.314462618e3;
 struct Blob {
   std::vector<unsigned char> bytes;
   template <class T>
-  size_t add(const std::vector<T> &v) {
-    size_t off = (bytes.size() + 255) & ~size_t(255);
+  size_t add(const std::vector<T> &v, size_t align = 256) {
+    size_t off = (bytes.size() + align - 1) & ~(align - 1);
     bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 16), 0);
     if (!v.empty()) std::memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
     return off;
@@ -181,29 +181,39 @@ DeviceMechanism::DeviceMechanism(const MechTables &t, const JacPattern &p) {
   }
   const std::vector<int> rxn_order = sorted_by(rc), spc_order = sorted_by(sc2), col_order = sorted_by(cc);
 
-  Blob b;
-  size_t o_mw = b.add(t.mw), o_imw = b.add(inv_mw), o_rimw = b.add(ru_inv_mw), o_th = b.add(t.thermo);
-  size_t o_rec = b.add(rec);
-  size_t o_tbp = b.add(t.tb_ptr), o_tbs = b.add(t.tb_spc), o_tba = b.add(t.tb_alpha);
-  size_t o_fop = b.add(t.fo_ptr), o_foe = b.add(t.fo_eff_spc), o_fot = b.add(t.fo_type),
-         o_fos = b.add(t.fo_spc), o_foa = b.add(t.fo_alpha), o_fopar = b.add(t.fo_par);
-  size_t o_plpp = b.add(t.plog_pt_ptr), o_pllp = b.add(t.plog_ln_ptr), o_plp = b.add(t.plog_p),
-         o_pllnp = b.add(t.plog_lnp), o_pla = b.add(t.plog_lnA), o_pls = b.add(t.plog_sgn),
-         o_pln = b.add(t.plog_n), o_plt = b.add(t.plog_Ta);
-  size_t o_sdp = b.add(sd_ptr), o_sds = b.add(sd_step), o_scp = b.add(sc_ptr), o_scs = b.add(sc_step);
-  size_t o_cp = b.add(p.col_ptr), o_ri = b.add(p.row_idx), o_lr = b.add(p.last_row);
-  size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
-  size_t o_jrp = b.add(jr_ptr), o_jrk = b.add(jr_kk), o_jrc = b.add(jr_col);
-  size_t o_jw = b.add(jw), o_jt = b.add(jt), o_jtp = b.add(jt_ptr), o_jc = b.add(jcost),
-         o_jf = b.add(jf_ptr);
-  size_t o_ro = b.add(rxn_order), o_so = b.add(spc_order), o_co = b.add(col_order);
+  // The tables of the rates kernel first, 16-byte aligned and contiguous:
+  // the kernel may stage [blob, blob + hot_bytes) in shared memory.
   std::vector<RxnRec> rec_by_cost;
   for (int p : rxn_order) rec_by_cost.push_back(rec[p]);
-  size_t o_rbc = b.add(rec_by_cost);
+  Blob b;
+  const size_t h = 16;
+  size_t o_rbc = b.add(rec_by_cost, h);
+  size_t o_mw = b.add(t.mw, h), o_imw = b.add(inv_mw, h), o_rimw = b.add(ru_inv_mw, h),
+         o_th = b.add(t.thermo, h);
+  size_t o_tbp = b.add(t.tb_ptr, h), o_tbs = b.add(t.tb_spc, h), o_tba = b.add(t.tb_alpha, h);
+  size_t o_fop = b.add(t.fo_ptr, h), o_foe = b.add(t.fo_eff_spc, h), o_fot = b.add(t.fo_type, h),
+         o_fos = b.add(t.fo_spc, h), o_foa = b.add(t.fo_alpha, h), o_fopar = b.add(t.fo_par, h);
+  size_t o_plpp = b.add(t.plog_pt_ptr, h), o_pllp = b.add(t.plog_ln_ptr, h), o_plp = b.add(t.plog_p, h),
+         o_pllnp = b.add(t.plog_lnp, h), o_pla = b.add(t.plog_lnA, h), o_pls = b.add(t.plog_sgn, h),
+         o_pln = b.add(t.plog_n, h), o_plt = b.add(t.plog_Ta, h);
+  size_t o_sdp = b.add(sd_ptr, h), o_sds = b.add(sd_step, h), o_scp = b.add(sc_ptr, h),
+         o_scs = b.add(sc_step, h);
+  size_t o_so = b.add(spc_order, h);
+  size_t o_cp = b.add(p.col_ptr, h), o_ri = b.add(p.row_idx, h);
+  size_t o_jw = b.add(jw, h), o_jt = b.add(jt, h), o_jtp = b.add(jt_ptr, h), o_jc = b.add(jcost, h),
+         o_jf = b.add(jf_ptr, h);
+  const size_t hot = (b.bytes.size() + 15) & ~size_t(15);
+  size_t o_rec = b.add(rec);
+  size_t o_lr = b.add(p.last_row);
+  size_t o_ndp = b.add(nzd_ptr), o_nds = b.add(nzd_step), o_ncp = b.add(nzc_ptr), o_ncs = b.add(nzc_step);
+  size_t o_jrp = b.add(jr_ptr), o_jrk = b.add(jr_kk), o_jrc = b.add(jr_col);
+  size_t o_ro = b.add(rxn_order), o_co = b.add(col_order);
   bytes_ = b.bytes.size();
   check(cudaMalloc(&blob_, bytes_), "cudaMalloc(mechanism tables)");
   check(cudaMemcpy(blob_, b.bytes.data(), bytes_, cudaMemcpyHostToDevice), "cudaMemcpy(mechanism tables)");
   auto P = [&](size_t off) { return (const void *)((const unsigned char *)blob_ + off); };
+  view_.base = (const unsigned char *)blob_;
+  view_.hot_bytes = (int)hot;
   view_.nsp = ns;
   view_.nrxn = t.nrxn;
   view_.nstep = t.nstep;

@@ -79,6 +79,11 @@ struct DevMech {
   // the reaction records in rxn_order order (position p holds reaction
   // rxn_order[p]): one load instead of two dependent ones per work item
   const RxnRec *rxn_by_cost;
+  // The tables the rates kernel reads form the first hot_bytes bytes of the
+  // allocation at base (16-byte aligned), so a CTA can stage them in shared
+  // memory and address them at a fixed offset from their global copies.
+  const unsigned char *base;
+  int hot_bytes;
 };
 
 // Host-side builder; owns the device allocation.

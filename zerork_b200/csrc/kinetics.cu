@@ -21,6 +21,7 @@
 //                        difference temperature column, dC->dY conversion).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 
 #include "devmech.h"
@@ -82,7 +83,8 @@ template <int TS, int V, int MAXT>
 __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     DevMech m, int n, int ld, const double *__restrict__ Tin, const double *__restrict__ Pin,
     const double *__restrict__ Y, double *__restrict__ wdot, double *__restrict__ jac,
-    double *__restrict__ ydot, KinParams kp, double *__restrict__ gscratch, int ws_doubles) {
+    double *__restrict__ ydot, KinParams kp, double *__restrict__ gscratch, int ws_doubles,
+    int stage_bytes) {
   constexpr int GS = TS / V;
   extern __shared__ double smem_dyn[];
   const int S = m.nsp, N = m.nstep;
@@ -94,6 +96,17 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
   const bool wlead = (threadIdx.x & 31) < GS;  // holds the warp partial
   const Layout L = make_layout(S, N, NW);
   double *ws = gscratch ? gscratch + (size_t)blockIdx.x * ws_doubles : smem_dyn;
+  // the mechanism's hot tables staged in shared memory after the workspace
+  // (stage_bytes > 0): every table read below goes to the copy at offset tofs
+  long long tofs = 0;
+  if (stage_bytes > 0) {
+    int4 *dst = reinterpret_cast<int4 *>(smem_dyn + (gscratch ? 0 : ws_doubles));
+    const int4 *src = reinterpret_cast<const int4 *>(m.base);
+    for (int i = threadIdx.x; i < stage_bytes / 16; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    tofs = reinterpret_cast<const char *>(dst) - reinterpret_cast<const char *>(m.base);
+  }
+#define TB(f) rb(m.f, tofs)
   double *sC = ws + L.rC * TS, *sU = ws + L.rU * TS, *sG = ws + L.rG * TS;
   double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS, *sStash = ws + L.rStash * TS;
 #define PT(a, ww, k) sPart[((a) * NW + (ww)) * TS + q + (k) * GS]
@@ -111,8 +124,8 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
   for (int rr_ = 0; rr_ * NG < m.nrxn; ++rr_) {                                      \
     const int rp_ = rr_ * NG + ((rr_ & 1) ? NG - 1 - g : g);                         \
     if (rp_ < m.nrxn)                                                                \
-      reaction_item<TS, V>(m, load_rxn(m.rxn_by_cost + rp_), q, CONC, sG, sROP, Tr, logT, invT, \
-                           lprt, CSUM, kp.lim);                                      \
+      reaction_item<TS, V>(m, load_rxn(TB(rxn_by_cost) + rp_), q, CONC, sG, sROP, Tr, logT, invT, \
+                           lprt, CSUM, kp.lim, nullptr, tofs);                                      \
   }
   const int ntiles = (n + TS - 1) / TS;
   const double dummy_y = 1.0 / S;
@@ -132,7 +145,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       double pa[V];
       FORV pa[k] = 0.0;
       for (int s = g; s < S; s += NG) {
-        const double iw = m.inv_mw[s];
+        const double iw = TB(inv_mw)[s];
         FORV pa[k] += yload(s, k) * iw;
       }
       FORV pa[k] = warp_group_sum<GS>(pa[k]);
@@ -166,8 +179,8 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       double pc[V], pcv[V];
       FORV pc[k] = pcv[k] = 0.0;
       for (int s = g; s < S; s += NG) {
-        const double *th = m.thermo + 16 * s;
-        const double iw = m.inv_mw[s], riw = m.ru_inv_mw[s];
+        const double *th = TB(thermo) + 16 * s;
+        const double iw = TB(inv_mw)[s], riw = TB(ru_inv_mw)[s];
         FORV {
           const double y = yload(s, k);
           const double c = (1.0 / v[k]) * iw * y;
@@ -208,12 +221,12 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     {
       double pe[V];
       FORV pe[k] = 0.0;
-      SNAKE(s, m.spc_order, S) {
+      SNAKE(s, TB(spc_order), S) {
         double des[V], cre[V];
         FORV des[k] = cre[k] = 0.0;
-        gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
-        gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
-        const double mws = m.mw[s];
+        gather_rop<TS, V>(sROP, TB(sd_step), TB(sd_ptr)[s], TB(sd_ptr)[s + 1], q, des);
+        gather_rop<TS, V>(sROP, TB(sc_step), TB(sc_ptr)[s], TB(sc_ptr)[s + 1], q, cre);
+        const double mws = TB(mw)[s];
         FORV {
           const double net = cre[k] - des[k];
           if (valid[k]) {
@@ -248,8 +261,8 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         double pc[V], pcv[V];
         FORV pc[k] = pcv[k] = 0.0;
         for (int s = g; s < S; s += NG) {
-          const double *th = m.thermo + 16 * s;
-          const double iw = m.inv_mw[s], riw = m.ru_inv_mw[s];
+          const double *th = TB(thermo) + 16 * s;
+          const double iw = TB(inv_mw)[s], riw = TB(ru_inv_mw)[s];
           FORV {
             const double yc = clamp_mass_fraction(yload(s, k), kp.mmf);
             const double c = (1.0 / v[k]) * iw * yc;
@@ -285,17 +298,17 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       {
         double pe[V];
         FORV pe[k] = 0.0;
-        SNAKE(s, m.spc_order, S) {
+        SNAKE(s, TB(spc_order), S) {
           double des[V], cre[V];
           FORV des[k] = cre[k] = 0.0;
-          gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
-          gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
+          gather_rop<TS, V>(sROP, TB(sd_step), TB(sd_ptr)[s], TB(sd_ptr)[s + 1], q, des);
+          gather_rop<TS, V>(sROP, TB(sc_step), TB(sc_ptr)[s], TB(sc_ptr)[s + 1], q, cre);
           FORV pe[k] += sU[s * TS + q + k * GS] * (cre[k] - des[k]) * v[k];
         }
         FORV pe[k] = warp_group_sum<GS>(pe[k]);
         if (wlead) FORV PT(0, w, k) = pe[k];
         for (int s = g; s < S; s += NG) {  // the unclamped concentrations again
-          const double iw = m.inv_mw[s];
+          const double iw = TB(inv_mw)[s];
           FORV sC[s * TS + q + k * GS] = (1.0 / v[k]) * iw * yload(s, k);
         }
       }
@@ -315,9 +328,9 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     {
       int NGj = NG < S + 1 ? NG : S + 1;
       if (NGj > 2 * NW + 1) NGj = 2 * NW + 1;
-      const int total = m.jcost[m.nj];
+      const int total = TB(jcost)[m.nj];
       double *sTP = sG;
-      auto group_of = [&](int f) { return (int)(((long long)m.jcost[f] * NGj) / total); };
+      auto group_of = [&](int f) { return (int)(((long long)TB(jcost)[f] * NGj) / total); };
       // the temperature derivative and heat capacity of the (clamped) state
       // wait in partial rows for the temperature-row pass (fewer live registers)
       if (g == 0) FORV {
@@ -330,7 +343,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           int lo = 0, hi = m.nj;
           while (lo < hi) {
             const int mid = (lo + hi) >> 1;
-            if ((long long)m.jcost[mid] * NGj >= thr) hi = mid;
+            if ((long long)TB(jcost)[mid] * NGj >= thr) hi = mid;
             else lo = mid + 1;
           }
           return lo;
@@ -340,42 +353,42 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           int j = 0, hi = S;  // the column holding f0: jf_ptr[j] <= f0 < jf_ptr[j+1]
           while (j < hi) {
             const int mid = (j + hi + 1) >> 1;
-            if (m.jf_ptr[mid] <= f0) j = mid;
+            if (TB(jf_ptr)[mid] <= f0) j = mid;
             else hi = mid - 1;
           }
-          int jend = m.jf_ptr[j + 1];
-          int t = m.jt_ptr[f0];
-          double t2[V], trow[V], wcol = m.inv_mw[j];
+          int jend = TB(jf_ptr)[j + 1];
+          int t = TB(jt_ptr)[f0];
+          double t2[V], trow[V], wcol = TB(inv_mw)[j];
           FORV {
-            t2[k] = m.mw[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
+            t2[k] = TB(mw)[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
             trow[k] = 0.0;
           }
           for (int f = f0; f < f1; ++f) {
             while (f == jend) {  // column j ends inside this share
               FORV sTP[(j + g) * TS + q + k * GS] = trow[k];
               ++j;
-              jend = m.jf_ptr[j + 1];
-              wcol = m.inv_mw[j];
+              jend = TB(jf_ptr)[j + 1];
+              wcol = TB(inv_mw)[j];
               FORV {
-                t2[k] = m.mw[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
+                t2[k] = TB(mw)[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
                 trow[k] = 0.0;
               }
             }
-            const int2 w = m.jw[f];
+            const int2 w = TB(jw)[f];
             const int row = w.x, nd = w.y & 0xffff, nc = w.y >> 16;
             double des[V], cre[V];
             FORV des[k] = cre[k] = 0.0;
             for (int e = 0; e < nd; ++e) {
-              const double *rp = sROP + m.jt[t + e] * TS + q;
+              const double *rp = sROP + TB(jt)[t + e] * TS + q;
               FORV des[k] += rp[k * GS];
             }
             t += nd;
             for (int e = 0; e < nc; ++e) {
-              const double *rp = sROP + m.jt[t + e] * TS + q;
+              const double *rp = sROP + TB(jt)[t + e] * TS + q;
               FORV cre[k] += rp[k * GS];
             }
             t += nc;
-            const double conv = m.mw[row] * wcol;
+            const double conv = TB(mw)[row] * wcol;
             FORV {
               // destruction terms first, then creation (SetupJacobianSparse order)
               const double val = (0.0 - des[k] * t2[k]) + cre[k] * t2[k];
@@ -390,7 +403,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           int j = 0, hi = S;
           while (j < hi) {
             const int mid = (j + hi + 1) >> 1;
-            if (m.jf_ptr[mid] <= f0) j = mid;
+            if (TB(jf_ptr)[mid] <= f0) j = mid;
             else hi = mid - 1;
           }
           FORV sTP[(j + g) * TS + q + k * GS] = 0.0;
@@ -400,7 +413,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       // temperature row of column j: the partials of groups group_of(first
       // item) .. group_of(last item), in group order
       for (int j = g; j < S; j += NG) {
-        const int g0 = group_of(m.jf_ptr[j]), g1 = group_of(m.jf_ptr[j + 1] - 1);
+        const int g0 = group_of(TB(jf_ptr)[j]), g1 = group_of(TB(jf_ptr)[j + 1] - 1);
         double tp[V];
         FORV tp[k] = 0.0;
 #pragma unroll 1
@@ -408,15 +421,15 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
           const double *pp = sTP + (j + gg) * TS + q;
           FORV tp[k] += pp[k * GS];
         }
-        const double *th = m.thermo + 16 * j;
-        const size_t kk = (size_t)(m.jf_ptr[j + 1] + j) * ld;
+        const double *th = TB(thermo) + 16 * j;
+        const size_t kk = (size_t)(TB(jf_ptr)[j + 1] + j) * ld;
         FORV {
           double Tk = yS[k] * kp.Tref;  // the clamped temperature of this state
           if (Tk > 1.0e4) Tk = 1.0e4;
-          const double cvj = (nasa_cp(th, Tk) - 1.0) * m.ru_inv_mw[j];
+          const double cvj = (nasa_cp(th, Tk) - 1.0) * TB(ru_inv_mw)[j];
           double tr = tp[k] * (kRu * yS[k]);
-          tr += sStash[q + k * GS] * cvj * m.mw[j];
-          tr *= m.inv_mw[j] * (-1.0 / sStash[TS + q + k * GS]);
+          tr += sStash[q + k * GS] * cvj * TB(mw)[j];
+          tr *= TB(inv_mw)[j] * (-1.0 / sStash[TS + q + k * GS]);
           if (valid[k]) jac[kk + st[k]] = tr;
         }
       }
@@ -438,8 +451,8 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
       double pcv[V];
       FORV pcv[k] = 0.0;
       for (int s = g; s < S; s += NG) {
-        const double *th = m.thermo + 16 * s;
-        const double riw = m.ru_inv_mw[s];
+        const double *th = TB(thermo) + 16 * s;
+        const double riw = TB(ru_inv_mw)[s];
         FORV {
           double cp, h, gg;
           nasa_cp_h_g(th, Tr[k], logT[k], &cp, &h, &gg);
@@ -463,11 +476,11 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     {
       double pe[V];
       FORV pe[k] = 0.0;
-      SNAKE(s, m.spc_order, S) {
+      SNAKE(s, TB(spc_order), S) {
         double des[V], cre[V];
         FORV des[k] = cre[k] = 0.0;
-        gather_rop<TS, V>(sROP, m.sd_step, m.sd_ptr[s], m.sd_ptr[s + 1], q, des);
-        gather_rop<TS, V>(sROP, m.sc_step, m.sc_ptr[s], m.sc_ptr[s + 1], q, cre);
+        gather_rop<TS, V>(sROP, TB(sd_step), TB(sd_ptr)[s], TB(sd_ptr)[s + 1], q, des);
+        gather_rop<TS, V>(sROP, TB(sc_step), TB(sc_ptr)[s], TB(sc_ptr)[s + 1], q, cre);
         FORV {
           const double net = cre[k] - des[k];
           pe[k] += sU[s * TS + q + k * GS] * net * v[k];
@@ -485,13 +498,13 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
         for (int ww = 0; ww < NW; ++ww) es += PT(0, ww, k);
         tdp[k] = -es * kRu * ysp[k] / cvp[k] + 0.0;
       }
-      const int k0 = m.col_ptr[S], k1 = m.col_ptr[S + 1];
+      const int k0 = TB(col_ptr)[S], k1 = TB(col_ptr)[S + 1];
       for (int kk = k0 + g; kk < k1; kk += NG) {
-        const int row = m.row_idx[kk];
+        const int row = TB(row_idx)[kk];
         FORV {
           double d;
           if (row < S) {
-            const double mr = m.mw[row];
+            const double mr = TB(mw)[row];
             const double f1 = sU[row * TS + q + k * GS] * mr * v[k];
             const double f0 = (valid[k] ? wdot[(size_t)row * ld + st[k]] : 0.0) * mr * v[k];
             d = (f1 - f0) * mult[k];
@@ -505,6 +518,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     __syncthreads();
   }
 #undef PT
+#undef TB
 #undef FORV
 #undef SNAKE
 #undef RXN_PASS
@@ -518,25 +532,38 @@ cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams 
   const size_t ws_bytes = (size_t)L.rows * TS * sizeof(double);
   const int ntiles = (a.n + TS - 1) / TS;
   if (ntiles == 0) return cudaSuccess;
+  const int stage_bytes = cfg.stage ? m.hot_bytes : 0;
+  const size_t smem = (cfg.global_ws ? 0 : ws_bytes) + stage_bytes;
+  if (smem > 227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // the smallest shared-memory carve-out that holds the workspace (and the
+  // staged tables), so the rest of the SM's 256 KB stays L1
+  const int pct = (int)((100 * (smem + 1024) + 228 * 1024 - 1) / (228 * 1024));
+  e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           pct < 100 ? pct : 100);
+  if (e != cudaSuccess) return e;
   if (!cfg.global_ws) {
-    cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ws_bytes);
-    if (e != cudaSuccess) return e;
-    // the smallest shared-memory carve-out that holds the workspace, so the
-    // rest of the SM's 256 KB stays L1 for the mechanism tables
-    const int pct = (int)((100 * (ws_bytes + 1024) + 228 * 1024 - 1) / (228 * 1024));
-    e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
-                             cudaFuncAttributePreferredSharedMemoryCarveout, pct < 100 ? pct : 100);
-    if (e != cudaSuccess) return e;
-    rates_jac_kernel<TS, V, MAXT><<<ntiles, threads, ws_bytes, stream>>>(
-        m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac, a.ydot, kp, nullptr, 0);
+    // persistent CTAs when the tables are staged (one copy per CTA, not per tile)
+    int grid = ntiles;
+    if (cfg.stage) {
+      int dev = 0, sms = 148, per_sm = 1;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rates_jac_kernel<TS, V, MAXT>, threads, smem);
+      grid = std::min(ntiles, sms * std::max(1, per_sm));
+    }
+    rates_jac_kernel<TS, V, MAXT><<<grid, threads, smem, stream>>>(
+        m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac, a.ydot, kp, nullptr, (int)(ws_bytes / sizeof(double)),
+        stage_bytes);
   } else {
     int grid = cfg.grid > 0 ? cfg.grid : ntiles;
     if (grid > ntiles) grid = ntiles;
     if ((size_t)grid * ws_bytes > a.scratch_bytes) return cudaErrorInvalidValue;
-    rates_jac_kernel<TS, V, MAXT><<<grid, threads, 0, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
-                                                         a.jac, a.ydot, kp, a.scratch,
-                                                         (int)(ws_bytes / sizeof(double)));
+    rates_jac_kernel<TS, V, MAXT><<<grid, threads, smem, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
+                                                            a.jac, a.ydot, kp, a.scratch,
+                                                            (int)(ws_bytes / sizeof(double)), stage_bytes);
   }
   return cudaGetLastError();
 }
@@ -558,6 +585,10 @@ cudaError_t launch_tv(const DevMech &m, const RatesJacArgs &a, const KinParams &
 size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg) {
   const Layout L = make_layout(m.nsp, m.nstep, cfg.warps);
   return (size_t)L.rows * cfg.ts * sizeof(double);
+}
+
+size_t rates_jac_smem_bytes(const DevMech &m, const LaunchCfg &cfg) {
+  return (cfg.global_ws ? 0 : rates_jac_ws_bytes(m, cfg)) + (cfg.stage ? (size_t)m.hot_bytes : 0);
 }
 
 bool rates_jac_mapping_ok(const LaunchCfg &c) {

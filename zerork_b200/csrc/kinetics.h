@@ -25,6 +25,7 @@ struct LaunchCfg {
   int warps = 8;
   bool global_ws = false;
   int grid = 0;
+  bool stage = false;  // mechanism tables staged in each CTA's shared memory
 };
 
 // Species-major arrays x[item * ld + state]; ld >= n.
@@ -51,6 +52,9 @@ size_t rates_tc_smem_bytes(const DevMech &m, int ts, int threads);
 cudaError_t launch_rates_tc(const DevMech &m, const RatesTCArgs &a, cudaStream_t stream);
 
 size_t rates_jac_ws_bytes(const DevMech &m, const LaunchCfg &cfg);
+// Dynamic shared memory of a launch: the workspace (unless global) plus the
+// staged tables (cfg.stage).
+size_t rates_jac_smem_bytes(const DevMech &m, const LaunchCfg &cfg);
 bool rates_jac_mapping_ok(const LaunchCfg &cfg);
 cudaError_t launch_rates_jac(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
                              const LaunchCfg &cfg, cudaStream_t stream);

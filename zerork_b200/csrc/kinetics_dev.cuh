@@ -12,6 +12,14 @@ namespace zrk {
 constexpr double kRuD = 8.314462618e3;  // src/zerork/constants.h:10
 constexpr double kPatmD = 1.01325e5;    // src/zerork/constants.h:12
 
+// A table pointer moved by td bytes: the table's copy in shared memory when
+// the kernel staged the mechanism's hot tables (td = shared copy - global
+// base), the global table itself for td = 0.
+template <class T>
+__device__ __forceinline__ const T *rb(const T *p, long long td) {
+  return reinterpret_cast<const T *>(reinterpret_cast<const char *>(p) + td);
+}
+
 // NASA-7 polynomials (src/zerork/nasa_poly.cpp:50-172), one species, one T.
 __device__ __forceinline__ void nasa_cp_h_g(const double *__restrict__ c, double T, double logT,
                                             double *cp, double *h, double *g) {
@@ -45,37 +53,43 @@ __device__ __forceinline__ double nasa_cp(const double *__restrict__ c, double T
 // between the bracketing pressures inside; zero for T or P <= 0 or a
 // non-positive bracketing value (src/zerork/plog_reaction.cpp:166-300,
 // without extrapolation as rate_const.cpp:1174-1182 builds them).
-__device__ __forceinline__ double plog_at(const DevMech &m, int q, double invT, double logT) {
+__device__ __forceinline__ double plog_at(const DevMech &m, int q, double invT, double logT,
+                                          long long td = 0) {
+  const int *lp = rb(m.plog_ln_ptr, td);
+  const double *sg = rb(m.plog_sgn, td), *la = rb(m.plog_lnA, td), *ln = rb(m.plog_n, td),
+               *lt = rb(m.plog_Ta, td);
   double k = 0.0;
-  for (int l = m.plog_ln_ptr[q]; l < m.plog_ln_ptr[q + 1]; ++l)
-    k += m.plog_sgn[l] * exp(m.plog_lnA[l] + logT * m.plog_n[l] - invT * m.plog_Ta[l]);
+  for (int l = lp[q]; l < lp[q + 1]; ++l) k += sg[l] * exp(la[l] + logT * ln[l] - invT * lt[l]);
   return k;
 }
 
 static __device__ __forceinline__ double plog_rate(const DevMech &m, int j, double T, double invT, double logT,
-                                         double P) {
-  const int q0 = m.plog_pt_ptr[j], q1 = m.plog_pt_ptr[j + 1];
+                                         double P, long long td = 0) {
+  const int *pp = rb(m.plog_pt_ptr, td);
+  const double *pv = rb(m.plog_p, td), *lnp = rb(m.plog_lnp, td);
+  const int q0 = pp[j], q1 = pp[j + 1];
   if (T <= 0.0 || P <= 0.0) return 0.0;
-  if (q1 - q0 == 1 || P <= m.plog_p[q0]) return plog_at(m, q0, invT, logT);
-  if (P >= m.plog_p[q1 - 1]) return plog_at(m, q1 - 1, invT, logT);
+  if (q1 - q0 == 1 || P <= pv[q0]) return plog_at(m, q0, invT, logT, td);
+  if (P >= pv[q1 - 1]) return plog_at(m, q1 - 1, invT, logT, td);
   int r = q0;
-  while (r + 1 < q1 - 1 && !(m.plog_p[r] <= P && P < m.plog_p[r + 1])) ++r;
-  const double k1 = plog_at(m, r, invT, logT);
+  while (r + 1 < q1 - 1 && !(pv[r] <= P && P < pv[r + 1])) ++r;
+  const double k1 = plog_at(m, r, invT, logT, td);
   if (k1 <= 0.0) return 0.0;
-  const double k2 = plog_at(m, r + 1, invT, logT);
+  const double k2 = plog_at(m, r + 1, invT, logT, td);
   if (k2 <= 0.0) return 0.0;
-  const double e = log(k2 / k1) / (m.plog_lnp[r + 1] - m.plog_lnp[r]);
-  return k1 * pow(P / m.plog_p[r], e);
+  const double e = log(k2 / k1) / (lnp[r + 1] - lnp[r]);
+  return k1 * pow(P / pv[r], e);
 }
 
 // A reaction record read as six independent 16-byte loads: one memory round
-// trip instead of a chain of dependent field loads.
+// trip instead of a chain of dependent field loads (generic loads: the
+// record may sit in a staged shared-memory copy).
 __device__ __forceinline__ RxnRec load_rxn(const RxnRec *p) {
   static_assert(sizeof(RxnRec) == 96, "RxnRec layout");
   const int4 *src = reinterpret_cast<const int4 *>(p);
   int4 b[6];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) b[i] = __ldg(src + i);
+  for (int i = 0; i < 6; ++i) b[i] = src[i];
   RxnRec R;
   memcpy(&R, b, sizeof(R));
   return R;
@@ -93,12 +107,12 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
                                               const double *T, const double *logT,
                                               const double *invT, const double *lprt,
                                               const double *Csum, double lim,
-                                              const double *lim_step = nullptr) {
+                                              const double *lim_step = nullptr, long long td = 0) {
   constexpr int GS = TS / V;
   double kf[V], kr[V];
   if (R.flags & kPlog) {  // at the pressure of the concentrations, Csum Ru T (rate_const.cpp:548-567)
 #pragma unroll
-    for (int k = 0; k < V; ++k) kf[k] = plog_rate(m, R.aux, T[k], invT[k], logT[k], Csum[k] * kRuD * T[k]);
+    for (int k = 0; k < V; ++k) kf[k] = plog_rate(m, R.aux, T[k], invT[k], logT[k], Csum[k] * kRuD * T[k], td);
   } else {
 #pragma unroll
     for (int k = 0; k < V; ++k) kf[k] = exp(R.lnA + R.n * logT[k] - R.Ta * invT[k]);
@@ -132,13 +146,13 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
     for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
     // efficiencies four at a time: the table loads are independent of the
     // sums, which keep the list order
-    const int e0 = m.tb_ptr[R.aux], e1 = m.tb_ptr[R.aux + 1];
+    const int e0 = rb(m.tb_ptr, td)[R.aux], e1 = rb(m.tb_ptr, td)[R.aux + 1];
     int e = e0;
     for (; e + 3 < e1; e += 4) {
-      const double a0 = m.tb_alpha[e], a1 = m.tb_alpha[e + 1], a2 = m.tb_alpha[e + 2],
-                   a3 = m.tb_alpha[e + 3];
-      const double *c0 = sC + m.tb_spc[e] * TS + q, *c1 = sC + m.tb_spc[e + 1] * TS + q,
-                   *c2 = sC + m.tb_spc[e + 2] * TS + q, *c3 = sC + m.tb_spc[e + 3] * TS + q;
+      const double a0 = rb(m.tb_alpha, td)[e], a1 = rb(m.tb_alpha, td)[e + 1], a2 = rb(m.tb_alpha, td)[e + 2],
+                   a3 = rb(m.tb_alpha, td)[e + 3];
+      const double *c0 = sC + rb(m.tb_spc, td)[e] * TS + q, *c1 = sC + rb(m.tb_spc, td)[e + 1] * TS + q,
+                   *c2 = sC + rb(m.tb_spc, td)[e + 2] * TS + q, *c3 = sC + rb(m.tb_spc, td)[e + 3] * TS + q;
 #pragma unroll
       for (int k = 0; k < V; ++k) {
         Cm[k] += c0[k * GS] * a0;
@@ -148,8 +162,8 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
       }
     }
     for (; e < e1; ++e) {
-      const double a = m.tb_alpha[e];
-      const double *cp = sC + m.tb_spc[e] * TS + q;
+      const double a = rb(m.tb_alpha, td)[e];
+      const double *cp = sC + rb(m.tb_spc, td)[e] * TS + q;
 #pragma unroll
       for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
     }
@@ -161,9 +175,9 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
   }
   if (R.flags & kFalloff) {
     const int f = R.aux;
-    const double *p = m.fo_par + 8 * f;
-    const int fs = m.fo_spc[f];
-    const int ty = m.fo_type[f];
+    const double *p = rb(m.fo_par, td) + 8 * f;
+    const int fs = rb(m.fo_spc, td)[f];
+    const int ty = rb(m.fo_type, td)[f];
     double Cm[V];
     if (fs >= 0) {
 #pragma unroll
@@ -171,13 +185,13 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
     } else {
 #pragma unroll
       for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
-      const int e0 = m.fo_ptr[f], e1 = m.fo_ptr[f + 1];
+      const int e0 = rb(m.fo_ptr, td)[f], e1 = rb(m.fo_ptr, td)[f + 1];
       int e = e0;
       for (; e + 3 < e1; e += 4) {
-        const double a0 = m.fo_alpha[e], a1 = m.fo_alpha[e + 1], a2 = m.fo_alpha[e + 2],
-                     a3 = m.fo_alpha[e + 3];
-        const double *c0 = sC + m.fo_spc_eff[e] * TS + q, *c1 = sC + m.fo_spc_eff[e + 1] * TS + q,
-                     *c2 = sC + m.fo_spc_eff[e + 2] * TS + q, *c3 = sC + m.fo_spc_eff[e + 3] * TS + q;
+        const double a0 = rb(m.fo_alpha, td)[e], a1 = rb(m.fo_alpha, td)[e + 1], a2 = rb(m.fo_alpha, td)[e + 2],
+                     a3 = rb(m.fo_alpha, td)[e + 3];
+        const double *c0 = sC + rb(m.fo_spc_eff, td)[e] * TS + q, *c1 = sC + rb(m.fo_spc_eff, td)[e + 1] * TS + q,
+                     *c2 = sC + rb(m.fo_spc_eff, td)[e + 2] * TS + q, *c3 = sC + rb(m.fo_spc_eff, td)[e + 3] * TS + q;
 #pragma unroll
         for (int k = 0; k < V; ++k) {
           Cm[k] += c0[k * GS] * a0;
@@ -187,8 +201,8 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
         }
       }
       for (; e < e1; ++e) {
-        const double a = m.fo_alpha[e];
-        const double *cp = sC + m.fo_spc_eff[e] * TS + q;
+        const double a = rb(m.fo_alpha, td)[e];
+        const double *cp = sC + rb(m.fo_spc_eff, td)[e] * TS + q;
 #pragma unroll
         for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
       }
