@@ -56,6 +56,9 @@ def args_():
                    help="fraction of each config's reactor count (bounded calibration runs)")
     p.add_argument("--suite-pairs", type=int, default=1 << 20,
                    help="training pairs of the learned predictor in the suite")
+    p.add_argument("--integ-warm", type=int, default=1,
+                   help="1: time each batched form on a second call in the first call's cost order; "
+                        "0: one call per form, index order")
     p.add_argument("--plain-sample", type=int, default=256,
                    help="reactors the plain group path is timed on (a stratified sample)")
     p.add_argument("--integ-dt", type=float, default=2e-3,
@@ -360,7 +363,7 @@ def _ratios(res):
         res["chosen_over_plain"] = res["batched_fp32_learned"]["over_plain"]
 
 
-def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True, n_plain=1024):
+def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True, n_plain=1024, warm=True):
     """Reactors integrated/s on the 160-species / 900-reaction mechanism (2 ms
     per reactor at rtol 1e-8, atol 1e-20) through the cfd_plugin API with host
     arrays, one solve call per form on the same states in index order: the
@@ -405,10 +408,14 @@ def integration_bench(n_reactors, cpu=True, dt=2e-3, learned=True, n_plain=1024)
                 out[form]["sample"] = note
                 ends[form] = (idx, e)
             else:
-                out[form], e, c = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None)
+                out[form], e, c = _run_form(mf, tf, T, P, Y, dt, opts, net if use_net else None, warm=warm)
                 if form == "batched_fp64":
                     cost = c
                 ends[form] = (np.arange(n_reactors), e)
+            print(json.dumps({"progress": form, "reactors_per_s": out[form]["value"]}), file=sys.stderr,
+                  flush=True)
+        out["timing"] = ("second call in the first call's cost order" if warm
+                         else "one call per form, index order")
         _ratios(out)
         if cpu:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -492,6 +499,7 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None, n_plain=102
                 res["learned_predictor"] = {"pairs": int(Xp.shape[0]), "generate_s": t_gen,
                                             "train_s": time.perf_counter() - t0,
                                             "loss_first_last": [hist[0], hist[-1]]}
+                print(json.dumps({name: {"learned_predictor": res["learned_predictor"]}}), flush=True)
             dense = len(g.species) + 1 <= 256
             ends, cost = {}, None
             for form, opts, use_net in FORMS[1:] + FORMS[:1]:  # the plain path last
@@ -509,6 +517,7 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None, n_plain=102
                     if form == "batched_fp64":
                         cost = c
                     ends[form] = (np.arange(nr), e)
+                print(json.dumps({name: {form: res[form]}}), flush=True)
             sample = ends["plain_fp64"][0] if "plain_fp64" in ends else np.flatnonzero(cost > 0)
             if "plain_fp64" in res:
                 _ratios(res)
@@ -736,7 +745,7 @@ def main():
     integ = None
     if rank == 0 and world == 1 and a.reactors > 0:
         integ = integration_bench(a.reactors, cpu=not a.no_cpu, dt=a.integ_dt,
-                                  learned=not a.no_learned, n_plain=a.plain_sample)
+                                  learned=not a.no_learned, n_plain=a.plain_sample, warm=a.integ_warm != 0)
         # the small config (64 reactors, 10 species), where the plain group
         # path finishes: every form with its end-state verdict
         integ["c1"] = integration_suite(["c1"], pairs=1 << 16, warm=True)["c1"]

@@ -21,8 +21,8 @@
 namespace zrk {
 namespace {
 
-template <int TS, int V>
-__global__ void __launch_bounds__(256) rates_tc_kernel(DevMech m, int n, int ld,
+template <int TS, int V, int MINB>
+__global__ void __launch_bounds__(256, MINB) rates_tc_kernel(DevMech m, int n, int ld,
                                                       const double *__restrict__ Tin,
                                                       const double *__restrict__ Cin,
                                                       const double *__restrict__ lim_step,
@@ -76,10 +76,16 @@ __global__ void __launch_bounds__(256) rates_tc_kernel(DevMech m, int n, int ld,
       for (int ww = 0; ww < NW; ++ww) cs += sPart[ww * TS + q + k * GS];
       Csum[k] = cs;
     }
-    // reactions: both steps of each reaction
-    for (int r = g; r < m.nrxn; r += NG)
-      reaction_item<TS, V>(m, load_rxn(m.rxn + r), q, sC, sG, sROP, T, logT, invT, lprt, Csum, 0.0,
-                           lim_step);
+    // reactions: both steps of each reaction, the cost-sorted records dealt
+    // to the groups in snake order (round r gives group g the record at
+    // r*NG + g, or r*NG + NG-1-g for odd r) so every group's work is close
+    // to the mean
+    for (int rr = 0; rr * NG < m.nrxn; ++rr) {
+      const int rp = rr * NG + ((rr & 1) ? NG - 1 - g : g);
+      if (rp < m.nrxn)
+        reaction_item<TS, V>(m, load_rxn(m.rxn_by_cost + rp), q, sC, sG, sROP, T, logT, invT, lprt, Csum,
+                             0.0, lim_step);
+    }
     __syncthreads();
     // destruction and creation in ascending step order, net = create - destroy
     for (int s = g; s < S; s += NG) {
@@ -107,11 +113,11 @@ __global__ void __launch_bounds__(256) rates_tc_kernel(DevMech m, int n, int ld,
 #undef FORV
 }
 
-template <int TS, int V>
+template <int TS, int V, int MINB>
 cudaError_t launch_tv(const DevMech &m, const RatesTCArgs &a, int threads, cudaStream_t stream) {
   const int NW = threads / 32;
   const size_t bytes = ((size_t)(2 * m.nsp + m.nstep) * TS + (size_t)NW * TS) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(rates_tc_kernel<TS, V>,
+  cudaError_t e = cudaFuncSetAttribute(rates_tc_kernel<TS, V, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 148;
@@ -119,7 +125,7 @@ cudaError_t launch_tv(const DevMech &m, const RatesTCArgs &a, int threads, cudaS
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int ntiles = (a.n + TS - 1) / TS;
   const int grid = ntiles < 8 * sms ? ntiles : 8 * sms;
-  rates_tc_kernel<TS, V><<<grid, threads, bytes, stream>>>(m, a.n, a.ld, a.T, a.C, a.lim_step,
+  rates_tc_kernel<TS, V, MINB><<<grid, threads, bytes, stream>>>(m, a.n, a.ld, a.T, a.C, a.lim_step,
                                                           a.net, a.create, a.destroy, a.rop);
   return cudaGetLastError();
 }
@@ -132,11 +138,14 @@ size_t rates_tc_smem_bytes(const DevMech &m, int ts, int threads) {
 
 cudaError_t launch_rates_tc(const DevMech &m, const RatesTCArgs &a, cudaStream_t stream) {
   if (a.n <= 0) return cudaSuccess;
-  // 32 states per tile where the workspace fits in shared memory, else 16 or 8
-  const size_t kMax = 227 * 1024;
-  if (rates_tc_smem_bytes(m, 32, 256) <= kMax) return launch_tv<32, 2>(m, a, 256, stream);
-  if (rates_tc_smem_bytes(m, 16, 256) <= kMax) return launch_tv<16, 1>(m, a, 256, stream);
-  if (rates_tc_smem_bytes(m, 8, 256) <= kMax) return launch_tv<8, 1>(m, a, 256, stream);
+  // two 8-warp CTAs per SM (16 resident warps, 128 registers each) with 16
+  // states per tile where two workspaces fit in shared memory; else one CTA
+  // per SM with the largest tile that fits
+  const size_t kMax = 227 * 1024, kSm = 228 * 1024;
+  if (2 * (rates_tc_smem_bytes(m, 16, 256) + 1024) <= kSm) return launch_tv<16, 2, 2>(m, a, 256, stream);
+  if (rates_tc_smem_bytes(m, 32, 256) <= kMax) return launch_tv<32, 2, 1>(m, a, 256, stream);
+  if (rates_tc_smem_bytes(m, 16, 256) <= kMax) return launch_tv<16, 1, 1>(m, a, 256, stream);
+  if (rates_tc_smem_bytes(m, 8, 256) <= kMax) return launch_tv<8, 1, 1>(m, a, 256, stream);
   return cudaErrorInvalidValue;
 }
 
