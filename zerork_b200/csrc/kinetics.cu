@@ -79,7 +79,7 @@ __device__ __forceinline__ void gather_rop(const double *__restrict__ sROP, cons
   }
 }
 
-template <int TS, int V, int MAXT>
+template <int TS, int V, int MAXT, bool STAGE>
 __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     DevMech m, int n, int ld, const double *__restrict__ Tin, const double *__restrict__ Pin,
     const double *__restrict__ Y, double *__restrict__ wdot, double *__restrict__ jac,
@@ -96,17 +96,18 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
   const bool wlead = (threadIdx.x & 31) < GS;  // holds the warp partial
   const Layout L = make_layout(S, N, NW);
   double *ws = gscratch ? gscratch + (size_t)blockIdx.x * ws_doubles : smem_dyn;
-  // the mechanism's hot tables staged in shared memory after the workspace
-  // (stage_bytes > 0): every table read below goes to the copy at offset tofs
-  long long tofs = 0;
-  if (stage_bytes > 0) {
+  // STAGE: the mechanism's hot tables (stage_bytes of them) copied into
+  // shared memory after the workspace; every table read below goes to the
+  // copy (tab) instead of global memory
+  const char *tab = nullptr;
+  if constexpr (STAGE) {
     int4 *dst = reinterpret_cast<int4 *>(smem_dyn + (gscratch ? 0 : ws_doubles));
     const int4 *src = reinterpret_cast<const int4 *>(m.base);
     for (int i = threadIdx.x; i < stage_bytes / 16; i += blockDim.x) dst[i] = src[i];
     __syncthreads();
-    tofs = reinterpret_cast<const char *>(dst) - reinterpret_cast<const char *>(m.base);
+    tab = reinterpret_cast<const char *>(dst);
   }
-#define TB(f) rb(m.f, tofs)
+#define TB(f) rb(m.f, tab, m.base)
   double *sC = ws + L.rC * TS, *sU = ws + L.rU * TS, *sG = ws + L.rG * TS;
   double *sROP = ws + L.rROP * TS, *sPart = ws + L.rPart * TS, *sStash = ws + L.rStash * TS;
 #define PT(a, ww, k) sPart[((a) * NW + (ww)) * TS + q + (k) * GS]
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
     const int rp_ = rr_ * NG + ((rr_ & 1) ? NG - 1 - g : g);                         \
     if (rp_ < m.nrxn)                                                                \
       reaction_item<TS, V>(m, load_rxn(TB(rxn_by_cost) + rp_), q, CONC, sG, sROP, Tr, logT, invT, \
-                           lprt, CSUM, kp.lim, nullptr, tofs);                                      \
+                           lprt, CSUM, kp.lim, nullptr, tab);                                      \
   }
   const int ntiles = (n + TS - 1) / TS;
   const double dummy_y = 1.0 / S;
@@ -524,48 +525,61 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
 #undef RXN_PASS
 }
 
-template <int TS, int V, int MAXT>
-cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
-                       const LaunchCfg &cfg, cudaStream_t stream) {
+template <int TS, int V, int MAXT, bool STAGE>
+cudaError_t launch_tvms(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
+                        const LaunchCfg &cfg, cudaStream_t stream) {
   const int threads = cfg.warps * 32;
   const Layout L = make_layout(m.nsp, m.nstep, cfg.warps);
   const size_t ws_bytes = (size_t)L.rows * TS * sizeof(double);
   const int ntiles = (a.n + TS - 1) / TS;
   if (ntiles == 0) return cudaSuccess;
-  const int stage_bytes = cfg.stage ? m.hot_bytes : 0;
+  const int stage_bytes = STAGE ? m.hot_bytes : 0;
   const size_t smem = (cfg.global_ws ? 0 : ws_bytes) + stage_bytes;
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>,
+  cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT, STAGE>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // the smallest shared-memory carve-out that holds the workspace (and the
   // staged tables), so the rest of the SM's 256 KB stays L1
   const int pct = (int)((100 * (smem + 1024) + 228 * 1024 - 1) / (228 * 1024));
-  e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT, STAGE>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            pct < 100 ? pct : 100);
   if (e != cudaSuccess) return e;
   if (!cfg.global_ws) {
     // persistent CTAs when the tables are staged (one copy per CTA, not per tile)
     int grid = ntiles;
-    if (cfg.stage) {
+    if (STAGE) {
       int dev = 0, sms = 148, per_sm = 1;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rates_jac_kernel<TS, V, MAXT>, threads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rates_jac_kernel<TS, V, MAXT, STAGE>, threads, smem);
       grid = std::min(ntiles, sms * std::max(1, per_sm));
     }
-    rates_jac_kernel<TS, V, MAXT><<<grid, threads, smem, stream>>>(
+    rates_jac_kernel<TS, V, MAXT, STAGE><<<grid, threads, smem, stream>>>(
         m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac, a.ydot, kp, nullptr, (int)(ws_bytes / sizeof(double)),
         stage_bytes);
   } else {
     int grid = cfg.grid > 0 ? cfg.grid : ntiles;
     if (grid > ntiles) grid = ntiles;
     if ((size_t)grid * ws_bytes > a.scratch_bytes) return cudaErrorInvalidValue;
-    rates_jac_kernel<TS, V, MAXT><<<grid, threads, smem, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
+    rates_jac_kernel<TS, V, MAXT, STAGE><<<grid, threads, smem, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
                                                             a.jac, a.ydot, kp, a.scratch,
                                                             (int)(ws_bytes / sizeof(double)), stage_bytes);
   }
   return cudaGetLastError();
+}
+
+// Staged tables only with tiles of at most 16 states (larger tiles leave no
+// room for them beside the workspace).
+template <int TS, int V, int MAXT>
+cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
+                       const LaunchCfg &cfg, cudaStream_t stream) {
+  if constexpr (TS <= 16) {
+    if (cfg.stage) return launch_tvms<TS, V, MAXT, true>(m, a, kp, cfg, stream);
+  } else {
+    if (cfg.stage) return cudaErrorInvalidValue;
+  }
+  return launch_tvms<TS, V, MAXT, false>(m, a, kp, cfg, stream);
 }
 
 // Up to 8 warps per CTA the kernel may use 255 registers per thread, up to

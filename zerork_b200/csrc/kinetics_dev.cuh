@@ -12,12 +12,18 @@ namespace zrk {
 constexpr double kRuD = 8.314462618e3;  // src/zerork/constants.h:10
 constexpr double kPatmD = 1.01325e5;    // src/zerork/constants.h:12
 
-// A table pointer moved by td bytes: the table's copy in shared memory when
-// the kernel staged the mechanism's hot tables (td = shared copy - global
-// base), the global table itself for td = 0.
+// A mechanism table as the kernel reads it: its copy in the CTA's shared
+// memory when the kernel staged the hot tables (tab = the copy of the block
+// that starts at the global base), the global table itself for tab = null.
+// The staged address is formed from the shared-memory pointer, not by
+// offsetting the global one: a pointer derived from a kernel parameter may
+// be compiled as a global-space access, which a shared address must not
+// reach.  With tab a compile-time null the select folds away.
 template <class T>
-__device__ __forceinline__ const T *rb(const T *p, long long td) {
-  return reinterpret_cast<const T *>(reinterpret_cast<const char *>(p) + td);
+__device__ __forceinline__ const T *rb(const T *p, const char *tab, const unsigned char *gbase) {
+  return tab ? reinterpret_cast<const T *>(
+                   tab + (reinterpret_cast<const char *>(p) - reinterpret_cast<const char *>(gbase)))
+             : p;
 }
 
 // NASA-7 polynomials (src/zerork/nasa_poly.cpp:50-172), one species, one T.
@@ -54,28 +60,28 @@ __device__ __forceinline__ double nasa_cp(const double *__restrict__ c, double T
 // non-positive bracketing value (src/zerork/plog_reaction.cpp:166-300,
 // without extrapolation as rate_const.cpp:1174-1182 builds them).
 __device__ __forceinline__ double plog_at(const DevMech &m, int q, double invT, double logT,
-                                          long long td = 0) {
-  const int *lp = rb(m.plog_ln_ptr, td);
-  const double *sg = rb(m.plog_sgn, td), *la = rb(m.plog_lnA, td), *ln = rb(m.plog_n, td),
-               *lt = rb(m.plog_Ta, td);
+                                          const char *tab = nullptr) {
+  const int *lp = rb(m.plog_ln_ptr, tab, m.base);
+  const double *sg = rb(m.plog_sgn, tab, m.base), *la = rb(m.plog_lnA, tab, m.base), *ln = rb(m.plog_n, tab, m.base),
+               *lt = rb(m.plog_Ta, tab, m.base);
   double k = 0.0;
   for (int l = lp[q]; l < lp[q + 1]; ++l) k += sg[l] * exp(la[l] + logT * ln[l] - invT * lt[l]);
   return k;
 }
 
 static __device__ __forceinline__ double plog_rate(const DevMech &m, int j, double T, double invT, double logT,
-                                         double P, long long td = 0) {
-  const int *pp = rb(m.plog_pt_ptr, td);
-  const double *pv = rb(m.plog_p, td), *lnp = rb(m.plog_lnp, td);
+                                         double P, const char *tab = nullptr) {
+  const int *pp = rb(m.plog_pt_ptr, tab, m.base);
+  const double *pv = rb(m.plog_p, tab, m.base), *lnp = rb(m.plog_lnp, tab, m.base);
   const int q0 = pp[j], q1 = pp[j + 1];
   if (T <= 0.0 || P <= 0.0) return 0.0;
-  if (q1 - q0 == 1 || P <= pv[q0]) return plog_at(m, q0, invT, logT, td);
-  if (P >= pv[q1 - 1]) return plog_at(m, q1 - 1, invT, logT, td);
+  if (q1 - q0 == 1 || P <= pv[q0]) return plog_at(m, q0, invT, logT, tab);
+  if (P >= pv[q1 - 1]) return plog_at(m, q1 - 1, invT, logT, tab);
   int r = q0;
   while (r + 1 < q1 - 1 && !(pv[r] <= P && P < pv[r + 1])) ++r;
-  const double k1 = plog_at(m, r, invT, logT, td);
+  const double k1 = plog_at(m, r, invT, logT, tab);
   if (k1 <= 0.0) return 0.0;
-  const double k2 = plog_at(m, r + 1, invT, logT, td);
+  const double k2 = plog_at(m, r + 1, invT, logT, tab);
   if (k2 <= 0.0) return 0.0;
   const double e = log(k2 / k1) / (lnp[r + 1] - lnp[r]);
   return k1 * pow(P / pv[r], e);
@@ -107,12 +113,12 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
                                               const double *T, const double *logT,
                                               const double *invT, const double *lprt,
                                               const double *Csum, double lim,
-                                              const double *lim_step = nullptr, long long td = 0) {
+                                              const double *lim_step = nullptr, const char *tab = nullptr) {
   constexpr int GS = TS / V;
   double kf[V], kr[V];
   if (R.flags & kPlog) {  // at the pressure of the concentrations, Csum Ru T (rate_const.cpp:548-567)
 #pragma unroll
-    for (int k = 0; k < V; ++k) kf[k] = plog_rate(m, R.aux, T[k], invT[k], logT[k], Csum[k] * kRuD * T[k], td);
+    for (int k = 0; k < V; ++k) kf[k] = plog_rate(m, R.aux, T[k], invT[k], logT[k], Csum[k] * kRuD * T[k], tab);
   } else {
 #pragma unroll
     for (int k = 0; k < V; ++k) kf[k] = exp(R.lnA + R.n * logT[k] - R.Ta * invT[k]);
@@ -146,13 +152,13 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
     for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
     // efficiencies four at a time: the table loads are independent of the
     // sums, which keep the list order
-    const int e0 = rb(m.tb_ptr, td)[R.aux], e1 = rb(m.tb_ptr, td)[R.aux + 1];
+    const int e0 = rb(m.tb_ptr, tab, m.base)[R.aux], e1 = rb(m.tb_ptr, tab, m.base)[R.aux + 1];
     int e = e0;
     for (; e + 3 < e1; e += 4) {
-      const double a0 = rb(m.tb_alpha, td)[e], a1 = rb(m.tb_alpha, td)[e + 1], a2 = rb(m.tb_alpha, td)[e + 2],
-                   a3 = rb(m.tb_alpha, td)[e + 3];
-      const double *c0 = sC + rb(m.tb_spc, td)[e] * TS + q, *c1 = sC + rb(m.tb_spc, td)[e + 1] * TS + q,
-                   *c2 = sC + rb(m.tb_spc, td)[e + 2] * TS + q, *c3 = sC + rb(m.tb_spc, td)[e + 3] * TS + q;
+      const double a0 = rb(m.tb_alpha, tab, m.base)[e], a1 = rb(m.tb_alpha, tab, m.base)[e + 1], a2 = rb(m.tb_alpha, tab, m.base)[e + 2],
+                   a3 = rb(m.tb_alpha, tab, m.base)[e + 3];
+      const double *c0 = sC + rb(m.tb_spc, tab, m.base)[e] * TS + q, *c1 = sC + rb(m.tb_spc, tab, m.base)[e + 1] * TS + q,
+                   *c2 = sC + rb(m.tb_spc, tab, m.base)[e + 2] * TS + q, *c3 = sC + rb(m.tb_spc, tab, m.base)[e + 3] * TS + q;
 #pragma unroll
       for (int k = 0; k < V; ++k) {
         Cm[k] += c0[k * GS] * a0;
@@ -162,8 +168,8 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
       }
     }
     for (; e < e1; ++e) {
-      const double a = rb(m.tb_alpha, td)[e];
-      const double *cp = sC + rb(m.tb_spc, td)[e] * TS + q;
+      const double a = rb(m.tb_alpha, tab, m.base)[e];
+      const double *cp = sC + rb(m.tb_spc, tab, m.base)[e] * TS + q;
 #pragma unroll
       for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
     }
@@ -175,9 +181,9 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
   }
   if (R.flags & kFalloff) {
     const int f = R.aux;
-    const double *p = rb(m.fo_par, td) + 8 * f;
-    const int fs = rb(m.fo_spc, td)[f];
-    const int ty = rb(m.fo_type, td)[f];
+    const double *p = rb(m.fo_par, tab, m.base) + 8 * f;
+    const int fs = rb(m.fo_spc, tab, m.base)[f];
+    const int ty = rb(m.fo_type, tab, m.base)[f];
     double Cm[V];
     if (fs >= 0) {
 #pragma unroll
@@ -185,13 +191,13 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
     } else {
 #pragma unroll
       for (int k = 0; k < V; ++k) Cm[k] = Csum[k];
-      const int e0 = rb(m.fo_ptr, td)[f], e1 = rb(m.fo_ptr, td)[f + 1];
+      const int e0 = rb(m.fo_ptr, tab, m.base)[f], e1 = rb(m.fo_ptr, tab, m.base)[f + 1];
       int e = e0;
       for (; e + 3 < e1; e += 4) {
-        const double a0 = rb(m.fo_alpha, td)[e], a1 = rb(m.fo_alpha, td)[e + 1], a2 = rb(m.fo_alpha, td)[e + 2],
-                     a3 = rb(m.fo_alpha, td)[e + 3];
-        const double *c0 = sC + rb(m.fo_spc_eff, td)[e] * TS + q, *c1 = sC + rb(m.fo_spc_eff, td)[e + 1] * TS + q,
-                     *c2 = sC + rb(m.fo_spc_eff, td)[e + 2] * TS + q, *c3 = sC + rb(m.fo_spc_eff, td)[e + 3] * TS + q;
+        const double a0 = rb(m.fo_alpha, tab, m.base)[e], a1 = rb(m.fo_alpha, tab, m.base)[e + 1], a2 = rb(m.fo_alpha, tab, m.base)[e + 2],
+                     a3 = rb(m.fo_alpha, tab, m.base)[e + 3];
+        const double *c0 = sC + rb(m.fo_spc_eff, tab, m.base)[e] * TS + q, *c1 = sC + rb(m.fo_spc_eff, tab, m.base)[e + 1] * TS + q,
+                     *c2 = sC + rb(m.fo_spc_eff, tab, m.base)[e + 2] * TS + q, *c3 = sC + rb(m.fo_spc_eff, tab, m.base)[e + 3] * TS + q;
 #pragma unroll
         for (int k = 0; k < V; ++k) {
           Cm[k] += c0[k * GS] * a0;
@@ -201,8 +207,8 @@ __device__ __forceinline__ void reaction_item(const DevMech &m, const RxnRec &R,
         }
       }
       for (; e < e1; ++e) {
-        const double a = rb(m.fo_alpha, td)[e];
-        const double *cp = sC + rb(m.fo_spc_eff, td)[e] * TS + q;
+        const double a = rb(m.fo_alpha, tab, m.base)[e];
+        const double *cp = sC + rb(m.fo_spc_eff, tab, m.base)[e] * TS + q;
 #pragma unroll
         for (int k = 0; k < V; ++k) Cm[k] += cp[k * GS] * a;
       }
