@@ -487,7 +487,7 @@ def integration_suite(names, scale=1.0, pairs=1 << 20, threads=None, n_plain=102
             if learned:
                 from zerork_b200 import predictor as pr
                 t0 = time.perf_counter()
-                ng = max(64, min(4096, pairs // 64))
+                ng = max(64, min(16384, pairs // 64))  # 64 intervals of ng reactors
                 T0, P0, Y0 = mechgen.reactor_states(g, ng, "c3" if wl == "c5" else wl, seed=1001)
                 rounds = max(1, pairs // ng)
                 Xp, Tp = pr.generate_pairs(mf, tf, T0, P0, Y0, rounds=rounds, seed=5)
