@@ -43,7 +43,8 @@ def args_():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--launch", default="",
-                   help="ts,v,warps,global_ws: fixed rates-kernel mapping instead of the autotuner "
+                   help="ts,v,warps,flags (bit 0 global workspace, bit 1 staged tables, bit 2 two "
+                        "CTAs per SM): fixed rates-kernel mapping instead of the autotuner "
                         "(profiling captures of one known kernel)")
     p.add_argument("--reactors", type=int, default=4096,
                    help="reactors of the 160-species integration workload (0: skip)")
@@ -653,7 +654,7 @@ def main():
     # project autotuner: time every tile/warp mapping on the first 2^16 states
     if a.launch:
         ts, v, wp, flags = (int(x) for x in a.launch.split(","))
-        pm.set_launch(ts, v, wp, bool(flags & 1), 0, stage=bool(flags & 2))
+        pm.set_launch(ts, v, wp, bool(flags & 1), 0, stage=bool(flags & 2), two_ctas=bool(flags & 4))
         tuned_ms = None
     else:
         tuned, tuned_ms = pm.autotune(Td, Pd, Yd, W, J, n=min(n, 1 << 16), stream=sptr)

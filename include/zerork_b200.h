@@ -74,10 +74,13 @@ int zrk_mech_get_double_option(zrk_mech_t m, const char *name, double *value);
  * (ZRK_LAUNCH_GLOBAL_WS) puts the per-tile workspace in global scratch (grid
  * CTAs; 0 = one CTA per tile), bit 1 (ZRK_LAUNCH_STAGE_TABLES) copies the
  * mechanism tables the kernel reads into each CTA's shared memory beside
- * the workspace (rejected when the two do not fit).  ts = 0 restores the
- * default mapping. */
+ * the workspace (rejected when the two do not fit), bit 2
+ * (ZRK_LAUNCH_TWO_CTAS, up to 8 warps and 16 states per tile, tables not
+ * staged) compiles the kernel for two resident CTAs per SM (at most 128
+ * registers per thread).  ts = 0 restores the default mapping. */
 #define ZRK_LAUNCH_GLOBAL_WS 1
 #define ZRK_LAUNCH_STAGE_TABLES 2
+#define ZRK_LAUNCH_TWO_CTAS 4
 int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int flags, int grid);
 int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *flags, int *grid);
 

@@ -149,8 +149,8 @@ class Mechanism:
         check(lib().zrk_mech_get_double_option(self._h, name.encode(), C.byref(v)))
         return v.value
 
-    def set_launch(self, ts=0, v=1, warps=8, global_ws=False, grid=0, stage=False):
-        flags = (1 if global_ws else 0) | (2 if stage else 0)
+    def set_launch(self, ts=0, v=1, warps=8, global_ws=False, grid=0, stage=False, two_ctas=False):
+        flags = (1 if global_ws else 0) | (2 if stage else 0) | (4 if two_ctas else 0)
         check(lib().zrk_mech_set_launch(self._h, ts, v, warps, flags, grid))
 
     def get_launch(self):
@@ -158,7 +158,7 @@ class Mechanism:
         check(lib().zrk_mech_get_launch(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d),
                                         C.byref(e)))
         return dict(ts=a.value, v=b.value, warps=c.value, global_ws=bool(d.value & 1), grid=e.value,
-                    stage=bool(d.value & 2))
+                    stage=bool(d.value & 2), two_ctas=bool(d.value & 4))
 
     def autotune(self, T, P, Y, wdot, jac=None, n=None, stream=None):
         """Time every tile/warp mapping on a device sample; keep the fastest."""

@@ -224,8 +224,9 @@ int zrk_mech_set_launch(zrk_mech_t m, int ts, int v, int warps, int flags, int g
   c.warps = warps;
   c.global_ws = (flags & ZRK_LAUNCH_GLOBAL_WS) != 0;
   c.stage = (flags & ZRK_LAUNCH_STAGE_TABLES) != 0;
+  c.minb = (flags & ZRK_LAUNCH_TWO_CTAS) ? 2 : 1;
   c.grid = grid;
-  if (!rates_jac_mapping_ok(c) || grid < 0 || (flags & ~3))
+  if (!rates_jac_mapping_ok(c) || grid < 0 || (flags & ~7))
     return set_error(ZRK_ERR_INVALID_ARGUMENT, "bad launch mapping");
   if (rates_jac_smem_bytes(h->dev->view(), c) > 227 * 1024)
     return set_error(ZRK_ERR_INVALID_ARGUMENT, "workspace and staged tables do not fit in shared memory");
@@ -239,7 +240,9 @@ int zrk_mech_get_launch(zrk_mech_t m, int *ts, int *v, int *warps, int *flags, i
   if (ts) *ts = h->cfg.ts;
   if (v) *v = h->cfg.v;
   if (warps) *warps = h->cfg.warps;
-  if (flags) *flags = (h->cfg.global_ws ? ZRK_LAUNCH_GLOBAL_WS : 0) | (h->cfg.stage ? ZRK_LAUNCH_STAGE_TABLES : 0);
+  if (flags)
+    *flags = (h->cfg.global_ws ? ZRK_LAUNCH_GLOBAL_WS : 0) | (h->cfg.stage ? ZRK_LAUNCH_STAGE_TABLES : 0) |
+             (h->cfg.minb == 2 ? ZRK_LAUNCH_TWO_CTAS : 0);
   if (grid) *grid = h->cfg.grid;
   return ZRK_OK;
 }
@@ -271,25 +274,27 @@ int zrk_mech_autotune(zrk_mech_t m, int n, int ld, const double *T, const double
           c.global_ws = true;
           c.grid = 2 * sms;
         }
-        for (int stage = 0; stage < 2; ++stage) {
-        c.stage = stage != 0;
-        if (c.stage && rates_jac_smem_bytes(h->dev->view(), c) > 227 * 1024) continue;
-        h->cfg = c;
-        float t = 0.f;
-        bool ok = true;
-        for (int rep = 0; rep < 3 && ok; ++rep) {
-          cudaEventRecord(e0, st);
-          ok = zrk_rates_jac_dev(m, n, ld, T, P, Y, wdot, jac, nullptr, stream) == ZRK_OK;
-          cudaEventRecord(e1, st);
-          cudaEventSynchronize(e1);
-          float ms = 0.f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          if (rep > 0) t += ms;  // first launch warms up
-        }
-        if (ok && cudaGetLastError() == cudaSuccess && t < best_t) {
-          best_t = t;
-          best = c;
-        }
+        for (int variant = 0; variant < 3; ++variant) {
+          c.stage = variant == 1;
+          c.minb = variant == 2 ? 2 : 1;
+          if (c.stage && rates_jac_smem_bytes(h->dev->view(), c) > 227 * 1024) continue;
+          if (!rates_jac_mapping_ok(c)) continue;
+          h->cfg = c;
+          float t = 0.f;
+          bool ok = true;
+          for (int rep = 0; rep < 3 && ok; ++rep) {
+            cudaEventRecord(e0, st);
+            ok = zrk_rates_jac_dev(m, n, ld, T, P, Y, wdot, jac, nullptr, stream) == ZRK_OK;
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0) t += ms;  // first launch warms up
+          }
+          if (ok && cudaGetLastError() == cudaSuccess && t < best_t) {
+            best_t = t;
+            best = c;
+          }
         }
       }
   cudaEventDestroy(e0);

@@ -79,8 +79,8 @@ __device__ __forceinline__ void gather_rop(const double *__restrict__ sROP, cons
   }
 }
 
-template <int TS, int V, int MAXT, bool STAGE>
-__global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
+template <int TS, int V, int MAXT, bool STAGE, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) rates_jac_kernel(
     DevMech m, int n, int ld, const double *__restrict__ Tin, const double *__restrict__ Pin,
     const double *__restrict__ Y, double *__restrict__ wdot, double *__restrict__ jac,
     double *__restrict__ ydot, KinParams kp, double *__restrict__ gscratch, int ws_doubles,
@@ -525,7 +525,7 @@ __global__ void __launch_bounds__(MAXT, 1) rates_jac_kernel(
 #undef RXN_PASS
 }
 
-template <int TS, int V, int MAXT, bool STAGE>
+template <int TS, int V, int MAXT, bool STAGE, int MINB>
 cudaError_t launch_tvms(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
                         const LaunchCfg &cfg, cudaStream_t stream) {
   const int threads = cfg.warps * 32;
@@ -536,13 +536,13 @@ cudaError_t launch_tvms(const DevMech &m, const RatesJacArgs &a, const KinParams
   const int stage_bytes = STAGE ? m.hot_bytes : 0;
   const size_t smem = (cfg.global_ws ? 0 : ws_bytes) + stage_bytes;
   if (smem > 227 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT, STAGE>,
+  cudaError_t e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT, STAGE, MINB>,
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   // the smallest shared-memory carve-out that holds the workspace (and the
   // staged tables), so the rest of the SM's 256 KB stays L1
-  const int pct = (int)((100 * (smem + 1024) + 228 * 1024 - 1) / (228 * 1024));
-  e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT, STAGE>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  const int pct = (int)((100 * MINB * (smem + 1024) + 228 * 1024 - 1) / (228 * 1024));
+  e = cudaFuncSetAttribute(rates_jac_kernel<TS, V, MAXT, STAGE, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            pct < 100 ? pct : 100);
   if (e != cudaSuccess) return e;
   if (!cfg.global_ws) {
@@ -552,17 +552,17 @@ cudaError_t launch_tvms(const DevMech &m, const RatesJacArgs &a, const KinParams
       int dev = 0, sms = 148, per_sm = 1;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rates_jac_kernel<TS, V, MAXT, STAGE>, threads, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rates_jac_kernel<TS, V, MAXT, STAGE, MINB>, threads, smem);
       grid = std::min(ntiles, sms * std::max(1, per_sm));
     }
-    rates_jac_kernel<TS, V, MAXT, STAGE><<<grid, threads, smem, stream>>>(
+    rates_jac_kernel<TS, V, MAXT, STAGE, MINB><<<grid, threads, smem, stream>>>(
         m, a.n, a.ld, a.T, a.P, a.Y, a.wdot, a.jac, a.ydot, kp, nullptr, (int)(ws_bytes / sizeof(double)),
         stage_bytes);
   } else {
     int grid = cfg.grid > 0 ? cfg.grid : ntiles;
     if (grid > ntiles) grid = ntiles;
     if ((size_t)grid * ws_bytes > a.scratch_bytes) return cudaErrorInvalidValue;
-    rates_jac_kernel<TS, V, MAXT, STAGE><<<grid, threads, smem, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
+    rates_jac_kernel<TS, V, MAXT, STAGE, MINB><<<grid, threads, smem, stream>>>(m, a.n, a.ld, a.T, a.P, a.Y, a.wdot,
                                                             a.jac, a.ydot, kp, a.scratch,
                                                             (int)(ws_bytes / sizeof(double)), stage_bytes);
   }
@@ -575,11 +575,15 @@ template <int TS, int V, int MAXT>
 cudaError_t launch_tvm(const DevMech &m, const RatesJacArgs &a, const KinParams &kp,
                        const LaunchCfg &cfg, cudaStream_t stream) {
   if constexpr (TS <= 16) {
-    if (cfg.stage) return launch_tvms<TS, V, MAXT, true>(m, a, kp, cfg, stream);
+    if (cfg.stage) return launch_tvms<TS, V, MAXT, true, 1>(m, a, kp, cfg, stream);
+    if constexpr (MAXT == 256) {
+      if (cfg.minb == 2) return launch_tvms<TS, V, MAXT, false, 2>(m, a, kp, cfg, stream);
+    }
   } else {
     if (cfg.stage) return cudaErrorInvalidValue;
   }
-  return launch_tvms<TS, V, MAXT, false>(m, a, kp, cfg, stream);
+  if (cfg.minb != 1) return cudaErrorInvalidValue;
+  return launch_tvms<TS, V, MAXT, false, 1>(m, a, kp, cfg, stream);
 }
 
 // Up to 8 warps per CTA the kernel may use 255 registers per thread, up to
@@ -607,6 +611,7 @@ size_t rates_jac_smem_bytes(const DevMech &m, const LaunchCfg &cfg) {
 
 bool rates_jac_mapping_ok(const LaunchCfg &c) {
   if (c.warps < 1 || c.warps > 32) return false;
+  if (c.minb != 1 && (c.minb != 2 || c.warps > 8 || c.ts > 16 || c.stage)) return false;
   if (c.warps > 16 && c.v != 1) return false;  // 64 registers per thread: one state each
   switch (c.ts * 8 + c.v) {
     case 8 * 8 + 1: case 8 * 8 + 2: case 8 * 8 + 4:

@@ -26,6 +26,7 @@ struct LaunchCfg {
   bool global_ws = false;
   int grid = 0;
   bool stage = false;  // mechanism tables staged in each CTA's shared memory
+  int minb = 1;        // resident CTAs per SM the kernel is compiled for (1 or 2)
 };
 
 // Species-major arrays x[item * ld + state]; ld >= n.
