@@ -364,7 +364,10 @@ __global__ void __launch_bounds__(MAXT, MINB) rates_jac_kernel(
             t2[k] = TB(mw)[j] / clamp_mass_fraction(yload(j, k), kp.mmf) * v[k];
             trow[k] = 0.0;
           }
+          int2 wn = TB(jw)[f0];
           for (int f = f0; f < f1; ++f) {
+            const int2 w = wn;
+            if (f + 1 < f1) wn = TB(jw)[f + 1];  // the next item's record in flight during this one
             while (f == jend) {  // column j ends inside this share
               FORV sTP[(j + g) * TS + q + k * GS] = trow[k];
               ++j;
@@ -375,7 +378,6 @@ __global__ void __launch_bounds__(MAXT, MINB) rates_jac_kernel(
                 trow[k] = 0.0;
               }
             }
-            const int2 w = TB(jw)[f];
             const int row = w.x, nd = w.y & 0xffff, nc = w.y >> 16;
             double des[V], cre[V];
             FORV des[k] = cre[k] = 0.0;
